@@ -1,0 +1,316 @@
+"""Benchmark: ms per UPDC iteration on the 8 x 2048^2 -> 4096^2 workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload c1] [--form fp32|fp64|fp32-kahan|fp32-reference]
+
+A step is one iteration of the solver (updc/c_core/updc_core.c:1410-1456) on
+the workload's synthetic inputs, with everything already resident on the GPU.
+``value`` is the device time per iteration (CUDA events on the engine's
+stream, max over ranks), ``e2e`` the same through the public C ABI with the
+estimate uploaded from and read back to host memory every step.  The per-stage
+event timing pass gives the dominant kernel's roofline.  ``--impl reference``
+times the reference core itself (compiled from its sources with the FFTW-API
+shim, oracle/_ref) on the host cores for the same workload.
+Under torchrun (N > 1) every rank solves its own field (replicas: the path of
+one field does not shard without a collective).
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import json
+import math
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+
+# ----------------------------------------------------------------------------- helpers
+def env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.is_file():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def stage_bytes(w, fw, fh, links, tlinks, dtype_bytes=4):
+    """Algorithmic bytes of each kernel of one iteration (each input read once,
+    each output written once; complex = 2 x dtype_bytes)."""
+    N, W, H, nin, nout = w.nexp, w.W, w.H, w.iw * w.ih, w.W * w.H
+    M1 = fw // 2 + 1
+    c = 2 * dtype_bytes
+    spec_h = M1 * H * c          # a row-pass intermediate (u-major, H rows)
+    spec_f = M1 * fh * c         # a full spectrum (PSF OTF)
+    r = dtype_bytes
+    link_bytes = sum(4 * (nin + 1) + (4 * nin + 2 * L + (2 * L) % 4 if enc == 2 else 4 * L) + 4 * L
+                     for L, enc in links)
+    tmap_bytes = sum(4 * (nout + 1) + 8 * L for L in tlinks)
+    return {
+        "estimate_x_pass": nout * r + spec_h,
+        "forward_y_passes": spec_h + N * spec_f + N * spec_h,
+        "forward_x_pass": N * spec_h + N * nout * r,
+        "detector": link_bytes + N * (nin * r * 3 + nin * 2) + N * nout * r,
+        "adjoint_gather": tmap_bytes + N * nin * r + N * nout * r,
+        "scatter_x_pass": N * (nout * r + spec_h),
+        "adjoint_y_x_passes": N * spec_h + N * spec_f + spec_h + spec_h + nout * r,
+        "update": 4 * nout * r,
+    }
+
+
+STAGES = ["estimate_x_pass", "forward_y_passes", "forward_x_pass", "detector", "adjoint_gather",
+          "scatter_x_pass", "adjoint_y_x_passes", "update"]
+STAGE_LAUNCHES = {"estimate_x_pass": 1, "forward_y_passes": 1, "forward_x_pass": 1, "detector": 1,
+                  "adjoint_gather": 1, "scatter_x_pass": None, "adjoint_y_x_passes": 2, "update": 2}
+
+
+# ----------------------------------------------------------------------------- reference arm
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    from updc_b200 import synth
+    if not O.REF_BINARY.is_file():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/updc_jwst_c was not built"}))
+        return 0
+    cores = os.cpu_count() or 1
+    w = synth.WORKLOADS[args.workload]
+    workdir = Path(tempfile.mkdtemp(prefix="updc_bench_ref_"))
+    try:
+        ds = synth.generate(w.name, workdir)
+        # bounded sample: time one iteration first, then as many as fit ~150 s
+        fftw = max(1, cores // w.nexp)
+        def run(iters, prefix):
+            a = ds.engine_args(iterations=iters, prefix=prefix, fft_workers=fftw, exposure_workers=w.nexp,
+                               preprocess_workers=w.nexp).argv()
+            t0 = time.time()
+            r = subprocess.run([str(O.REF_BINARY), *a], capture_output=True, text=True,
+                               env={**os.environ, "UPDC_PERSIST_CACHE": "1"})
+            if r.returncode:
+                raise RuntimeError(r.stderr[-400:])
+            rows = list(csv.reader(open(f"{ds.directory}/{prefix}_timing.csv")))
+            its = [float(v) for k, v in rows[1:] if k.endswith("_total") and k.startswith("iteration_")]
+            return its, time.time() - t0
+        first, wall = run(1, "probe")       # also fills the reference's persistent caches
+        per = first[0]
+        total = args.warmup + args.steps
+        budget = max(1, int(150.0 / max(per, 1e-3)))
+        n = min(total, budget)
+        its, wall2 = run(n, "ref")
+        timed = its[min(args.warmup, n - 1):] if n > 1 else its
+        ms = 1000.0 * sum(timed) / len(timed)
+        sample = (f"{len(timed)} timed of {n} reference-core iterations on {args.workload} "
+                  f"({w.nexp}x{w.iw}x{w.ih} -> {w.W}x{w.H}), warm cache, fft_workers={fftw}, "
+                  f"exposure_workers={w.nexp}; FFT = project FFTW-API shim (FFTW3f absent)")
+        line = {"metric": "ms/iteration", "value": round(ms, 3), "unit": "ms", "n_gpus": world,
+                "steps": len(timed), "warmup": args.warmup, "ms_per_step": round(ms, 3),
+                "higher_is_better": False, "impl": "reference", "dtype": "f32", "data": "synthetic",
+                "config": {"workload": args.workload, "target": [w.W, w.H], "exposures": w.nexp,
+                           "detector": [w.iw, w.ih], "psf": w.psf_size},
+                "cpu_baseline": {"value": round(ms, 3), "unit": "ms", "cores": cores, "kind": "reference",
+                                 "sample": sample},
+                "e2e": {"value": round(ms, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+    finally:
+        shutil.rmtree(workdir, ignore_errors=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------- b200 arm
+def cpu_baseline_sample(ds, w):
+    """One iteration of the reference core on the same inputs (rank 0, N=1)."""
+    from oracle import oracle as O
+    if not O.REF_BINARY.is_file():
+        return None
+    cores = os.cpu_count() or 1
+    fftw = max(1, cores // w.nexp)
+    a = ds.engine_args(iterations=1, prefix="cpubase", fft_workers=fftw, exposure_workers=w.nexp,
+                       preprocess_workers=w.nexp).argv()
+    r = subprocess.run([str(O.REF_BINARY), *a], capture_output=True, text=True,
+                       env={**os.environ, "UPDC_PERSIST_CACHE": "1"}, timeout=900)
+    if r.returncode:
+        return {"value": None, "unit": "ms", "cores": cores, "kind": "reference", "sample": r.stderr[-200:]}
+    rows = list(csv.reader(open(f"{ds.directory}/cpubase_timing.csv")))
+    its = [float(v) for k, v in rows[1:] if k.startswith("iteration_") and k.endswith("_total")]
+    return {"value": round(1000.0 * its[0], 1), "unit": "ms", "cores": cores, "kind": "reference",
+            "sample": f"1 iteration of the reference core on the same {w.name} inputs "
+                      f"(fft_workers={fftw}, exposure_workers={w.nexp}, FFTW-API shim FFT)"}
+
+
+def b200_arm(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    from updc_b200 import synth
+    from updc_b200.engine import Engine
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local_rank))
+    w = synth.WORKLOADS[args.workload]
+    workdir = Path(args.data_dir or tempfile.mkdtemp(prefix=f"updc_bench_r{rank}_"))
+    ds = synth.generate(w.name, workdir, use_torch=True)
+    eng = Engine(form=args.form, device=local_rank)
+    eng.load(str(ds.manifest), w.W, w.H, w.iw, w.ih, w.nexp)
+    t0 = time.time()
+    eng.setup()
+    setup_s = time.time() - t0
+    fw, fh = eng.fft_shape
+    eng.iterate(args.warmup, check_each=False)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        t0 = time.time()
+        stats = eng.iterate(args.steps, check_each=False)
+        torch.cuda.synchronize()
+        wall = time.time() - t0
+    ms = 1000.0 * sum(s.seconds for s in stats) / len(stats)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    # per-stage pass (eager launches with events between stages)
+    eng.set_stage_timing(True)
+    st = eng.iterate(max(3, min(args.steps, 5)), check_each=False)
+    eng.set_stage_timing(False)
+    stage_ms = {name: 1000.0 * statistics.mean(s.stage_seconds[i] for s in st) for i, name in enumerate(STAGES)}
+    links = [(eng.link_count(k), eng.link_encoding(k)) for k in range(w.nexp)]
+    sb = stage_bytes(w, fw, fh, links, [L for L, _ in links], 8 if args.form == "fp64" else 4)
+    dom = max(stage_ms, key=stage_ms.get)
+    peak, peak_kind = measured_peaks()
+    achieved = sb[dom] / (stage_ms[dom] * 1e-3) / 1e9
+    # e2e through the C ABI with pinned host buffers: upload x, one iteration, read x back
+    xdt = torch.float64 if args.form == "fp64" else torch.float32
+    x = torch.empty((w.H, w.W), dtype=xdt, pin_memory=True).numpy()
+    eng.read_plane_into("estimate", x)
+    e2e_steps = max(2, min(args.steps, 5))
+    t0 = time.time()
+    for _ in range(e2e_steps):
+        eng.set_plane("estimate", x)
+        eng.iterate(1, check_each=True)
+        eng.read_plane_into("estimate", x)
+    e2e_ms = 1000.0 * (time.time() - t0) / e2e_steps
+    nout = w.W * w.H
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(ds, w)
+    launches_per_iter = 9 + w.nexp
+    result = {
+        "metric": "ms/iteration", "value": round(ms, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "form": args.form, "target": [w.W, w.H], "exposures": w.nexp,
+                   "detector": [w.iw, w.ih], "psf": w.psf_size, "fft": [fw, fh],
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "working set ~%.1f GB >> 126 MB L2; no flush needed" % (eng.device_bytes / 1e9)},
+        "wall_ms_per_step": round(1000.0 * wall / args.steps, 4),
+        "setup_s": round(setup_s, 2),
+        "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "algorithmic_bytes": sb[dom], "traffic": None},
+        "cpu_baseline": cpu,
+        "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": x.itemsize * nout,
+                "d2h_bytes_per_step": x.itemsize * nout},
+        "gpu_launches": launches_per_iter * args.steps,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(result))
+    eng.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if not args.data_dir:
+        shutil.rmtree(workdir, ignore_errors=True)
+    return 0
+
+
+def main():
+    p = argparse.ArgumentParser(description=__doc__)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--workload", default="c1")
+    p.add_argument("--form", default="fp32", choices=["fp32", "fp64", "fp32-kahan", "fp32-reference"])
+    p.add_argument("--data-dir", default=None)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    args = p.parse_args()
+    rank, world, local_rank = env_rank()
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+    return b200_arm(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,260 @@
+"""GPU parity of every stage of the B200 engine against the oracle, through the C ABI.
+
+Integer and ordered-FP32 stages are compared bit for bit (LinkMap bytes and
+decode, weight normalisation, drizzle, the detector loop and its adjoint
+gather, the update); FFT-based stages against the FP64 oracle with the
+tolerances written in each test; whole solves against the compiled
+reference core.
+"""
+from __future__ import annotations
+
+import csv
+import filecmp
+import shutil
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import fft_shape_for, rel_rms
+
+pytestmark = pytest.mark.gpu
+
+
+def _engine(ds, form="fp32", **kw):
+    from updc_b200.engine import Engine
+    w = ds.workload
+    e = Engine(form=form, **kw)
+    e.load(str(ds.manifest), w.W, w.H, w.iw, w.ih, w.nexp)
+    e.setup()
+    return e
+
+
+def _oracle_solver(oracle, ds, precision=32, fft_shape=None):
+    w = ds.workload
+    fw, fh = fft_shape or fft_shape_for(ds)
+    return oracle.Solver(str(ds.manifest), w.W, w.H, w.iw, w.ih, w.nexp, fw, fh, precision=precision)
+
+
+# ---------------------------------------------------------------------------- geometry / LinkMap
+def test_self_test_on_device(engine_lib):
+    from updc_b200.engine import self_test
+    assert "OK" in self_test()
+
+
+@pytest.mark.parametrize("name", ["small", "abs32", "c0", "medium"])
+def test_linkmap_build_byte_identical(engine_lib, oracle, datasets, name, tmp_path):
+    from updc_b200.engine import build_linkmap
+    ds = datasets(name)
+    w = ds.workload
+    for k, row in enumerate(ds.rows):
+        mine = tmp_path / f"gpu_{k}.links"
+        ref = tmp_path / f"orc_{k}.links"
+        nl, enc = build_linkmap(row.vertices, mine, w.iw, w.ih, w.W, w.H)
+        onl, oenc = oracle.linkmap_build(row.vertices, w.iw, w.ih, w.W, w.H, str(ref))
+        assert (nl, enc) == (onl, oenc)
+        assert filecmp.cmp(mine, ref, shallow=False), f"exposure {k}: LinkMap bytes differ"
+    if name == "abs32":
+        assert enc == 1
+
+
+@pytest.mark.parametrize("name", ["small", "abs32", "c0"])
+def test_linkmap_decode_bit_exact(engine_lib, oracle, datasets, name):
+    ds = datasets(name)
+    w = ds.workload
+    e = _engine(ds, form="fp32-reference")
+    for k, row in enumerate(ds.rows):
+        off, tgt, frac, enc = oracle.linkmap_decode(row.links, w.iw, w.ih, w.W, w.H)
+        assert e.link_encoding(k) == enc
+        assert e.link_count(k) == len(tgt)
+        np.testing.assert_array_equal(e.decode_links(k), tgt)
+
+
+# ---------------------------------------------------------------------------- setup stages
+@pytest.mark.parametrize("form", ["fp32-reference", "fp32"])
+def test_setup_planes_bit_exact(engine_lib, oracle, datasets, form):
+    """Weight scale, masked/normalised SCI/WHT, coverage and the drizzle x0."""
+    ds = datasets("c0")
+    e = _engine(ds, form=form)
+    s = _oracle_solver(oracle, ds)
+    assert np.float32(e.weight_scale) == np.float32(s.weight_scale)
+    for k in range(ds.workload.nexp):
+        np.testing.assert_array_equal(e.plane("science", k), s.sci[k])
+        np.testing.assert_array_equal(e.plane("weight", k), s.wht[k])
+    np.testing.assert_array_equal(e.plane("coverage"), s.coverage)
+    np.testing.assert_array_equal(e.plane("estimate"), s.estimate)
+
+
+@pytest.mark.parametrize("form,tol", [("fp32", 2e-6), ("fp32-reference", 2e-5), ("fp64", 1e-12)])
+def test_denominator_vs_fp64_oracle(engine_lib, oracle, datasets, form, tol):
+    """D = sum_k H_k^T W_k against the FP64 oracle (relative RMS <= tol)."""
+    ds = datasets("c0")
+    e = _engine(ds, form=form)
+    s64 = _oracle_solver(oracle, ds, precision=64)
+    d = e.plane("denominator", as_double=True)
+    assert rel_rms(d, s64.denominator) <= tol
+    assert abs(e.max_sensitivity - s64.max_sensitivity) <= 10 * tol * s64.max_sensitivity
+
+
+@pytest.mark.parametrize("form,tol", [("fp32", 2e-6), ("fp64", 1e-12)])
+def test_forward_model_vs_fp64_oracle(engine_lib, oracle, datasets, form, tol):
+    """blur_k = crop(C2R(R2C(pad(x)) K_k))/nf for every exposure (relative RMS <= tol)."""
+    ds = datasets("c0")
+    e = _engine(ds, form=form)
+    s64 = _oracle_solver(oracle, ds, precision=64)
+    e.set_plane("estimate", s64.estimate)
+    e.stage_forward()
+    for k in range(ds.workload.nexp):
+        ref = s64.forward_blur(k)
+        assert rel_rms(e.plane("blur", k, as_double=True), ref) <= tol
+
+
+# ---------------------------------------------------------------------------- detector / update
+@pytest.mark.parametrize("background", [None, -100.0])
+def test_detector_and_adjoint_gather_bit_exact(engine_lib, oracle, datasets, background):
+    """Same blur in, same scatter out: the fused detector loop, FreezeMu and the
+    target-major gather reproduce updc_core.c:1152-1177 bit for bit."""
+    ds = datasets("c0", background)
+    e = _engine(ds, form="fp32-reference")
+    s = _oracle_solver(oracle, ds)
+    blurs = [s.forward_blur(k) for k in range(ds.workload.nexp)]
+    for k, b in enumerate(blurs):
+        e.set_plane("blur", b, k)
+    new, tot, mn = e.stage_detector()
+    for k, b in enumerate(blurs):
+        sc, nn, nt, m = s.detector(k, b)
+        np.testing.assert_array_equal(e.plane("scatter", k), sc)
+        assert (int(new[k]), int(tot[k])) == (nn, nt)
+        assert np.float32(mn[k]) == np.float32(m)
+        np.testing.assert_array_equal(e.plane("frozen", k), s.frozen[k])
+    if background is not None:
+        assert int(tot.sum()) > 0
+
+
+def test_update_bit_exact(engine_lib, oracle, datasets):
+    ds = datasets("c0")
+    e = _engine(ds, form="fp32-reference")
+    s = _oracle_solver(oracle, ds)
+    x0 = s.estimate.copy()
+    s.iterate(1)
+    # feed the oracle's correction and denominator, start from the same x
+    e.set_plane("estimate", x0)
+    e.set_plane("correction", s.correction)
+    e.set_plane("denominator", s.denominator)
+    total, neg = e.stage_update()
+    np.testing.assert_array_equal(e.plane("estimate"), s.estimate)
+    assert neg == int((s.estimate < 0).sum())
+
+
+# ---------------------------------------------------------------------------- whole solves
+def _reference_run(ref_bin, ds, iterations, tmp_path, prefix="ref"):
+    args = ds.engine_args(iterations=iterations, prefix=prefix).argv()
+    r = subprocess.run([str(ref_bin), *args], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    w = ds.workload
+    x = np.fromfile(f"{ds.directory}/{prefix}_{iterations:02d}.bin", np.float32).reshape(w.H, w.W)
+    with open(f"{ds.directory}/{prefix}_mufreeze.csv") as f:
+        rows = list(csv.DictReader(f))
+    return x, rows
+
+
+@pytest.mark.parametrize("name", ["c0", "medium"])
+def test_fp32_solve_matches_reference(engine_lib, reference_binary, datasets, name, tmp_path):
+    """FP32 form after the workload's iterations within 1e-5 relative RMS of the reference core."""
+    ds = datasets(name)
+    w = ds.workload
+    xref, _ = _reference_run(reference_binary, ds, w.iterations, tmp_path)
+    e = _engine(ds, form="fp32")
+    e.iterate(w.iterations)
+    x = e.plane("estimate")
+    assert rel_rms(x, xref) <= 1e-5
+
+
+def test_fp64_solve_matches_fp64_oracle(engine_lib, oracle, datasets):
+    ds = datasets("c0")
+    w = ds.workload
+    s64 = _oracle_solver(oracle, ds, precision=64)
+    s64.iterate(w.iterations)
+    e = _engine(ds, form="fp64")
+    e.iterate(w.iterations)
+    assert rel_rms(e.plane("estimate", as_double=True), s64.estimate) <= 1e-12
+
+
+def test_forced_freeze_rows_match_reference(engine_lib, reference_binary, datasets, tmp_path):
+    """Background -100 (the reference smoke test's forced FreezeMu): per-iteration
+    freeze counts equal the reference core's and the totals accumulate."""
+    ds = datasets("c0", -100.0)
+    w = ds.workload
+    iters = 4
+    xref, rows = _reference_run(reference_binary, ds, iters, tmp_path)
+    e = _engine(ds, form="fp32-reference")
+    st = e.iterate(iters)
+    mine = [(int(s.new_frozen[k]), int(s.total_frozen[k])) for s in st for k in range(w.nexp)]
+    theirs = [(int(r["n_new_frozen"]), int(r["n_total_frozen"])) for r in rows]
+    mismatch = sum(abs(a[1] - b[1]) for a, b in zip(mine, theirs))
+    total = sum(b[1] for b in theirs)
+    assert total > 0
+    assert mismatch <= max(2, total // 1000), (mine, theirs)
+    for k in range(w.nexp):
+        assert st[0].total_frozen[k] == st[0].new_frozen[k]
+        assert st[1].total_frozen[k] == st[0].total_frozen[k] + st[1].new_frozen[k]
+
+
+def test_graph_and_eager_paths_identical(engine_lib, datasets):
+    """The CUDA-graph replay and eager launches give bit-identical results, and
+    two runs are bit-identical (no float atomics anywhere)."""
+    ds = datasets("c0")
+    outs = []
+    for graph in (True, False, True):
+        e = _engine(ds, form="fp32", use_graph=graph)
+        e.iterate(5, check_each=False)
+        outs.append(e.plane("estimate"))
+    np.testing.assert_array_equal(outs[0], outs[1])
+    np.testing.assert_array_equal(outs[0], outs[2])
+
+
+def test_dropin_executable(engine_lib, reference_binary, datasets, tmp_path):
+    """updc_b200/bin/updc_jwst_c with the 18-argument contract writes the
+    reference's outputs; the WHT product (coverage x weight scale) is
+    bit-identical and x is within 1e-5 relative RMS."""
+    from updc_b200 import _lib
+    ds = datasets("c0")
+    w = ds.workload
+    iters = 5
+    xref, rows_ref = _reference_run(reference_binary, ds, iters, tmp_path, prefix="refd")
+    args = ds.engine_args(iterations=iters, prefix="b200", save_every=2).argv()
+    r = subprocess.run([str(_lib.EXE_PATH), *args], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    d = Path(ds.directory)
+    assert (d / "b200_02.bin").is_file() and (d / "b200_04.bin").is_file() and (d / "b200_05.bin").is_file()
+    x = np.fromfile(d / "b200_05.bin", np.float32).reshape(w.H, w.W)
+    assert rel_rms(x, xref) <= 1e-5
+    wht = np.fromfile(d / "b200_wht.bin", np.float32)
+    wref = np.fromfile(d / "refd_wht.bin", np.float32)
+    np.testing.assert_array_equal(wht, wref)
+    with open(d / "b200_mufreeze.csv") as f:
+        rows = list(csv.DictReader(f))
+    assert len(rows) == iters * w.nexp
+    assert list(rows[0].keys()) == list(rows_ref[0].keys())
+    timing = (d / "b200_timing.csv").read_text().splitlines()
+    assert timing[0] == "stage,wall_seconds" and any(t.startswith(f"iteration_{iters:02d}_total") for t in timing)
+    st = subprocess.run([str(_lib.EXE_PATH), "--self-test"], capture_output=True, text=True)
+    assert st.returncode == 0
+
+
+def test_error_negative_yeff(engine_lib, datasets, tmp_path):
+    """A pedestal too small for the data fails setup with the reference's message."""
+    from updc_b200 import handoff
+    from updc_b200.engine import Engine, UpdcError
+    ds = datasets("small")
+    rows = [handoff.ExposureRow(**{**r.__dict__}) for r in ds.rows]
+    for r in rows:
+        r.pedestal = 0.0
+    m = tmp_path / "manifest_bad.txt"
+    handoff.write_manifest(m, rows)
+    w = ds.workload
+    e = Engine(form="fp32")
+    e.load(str(m), w.W, w.H, w.iw, w.ih, w.nexp)
+    with pytest.raises(UpdcError, match="negative/non-finite y_eff reached solver"):
+        e.setup()

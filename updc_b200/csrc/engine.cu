@@ -1,0 +1,974 @@
+// UPDC solver engine: setup stages and the per-iteration kernel sequence.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "engine.cuh"
+#include "fft.cuh"
+#include "kernels.cuh"
+#include "linkmap.cuh"
+#include "pointwise.cuh"
+
+namespace updc {
+
+const char *error_message(uint32_t code) {
+    switch (code) {
+        case ERR_NONFINITE_MEAN: return "non-finite forward mean";
+        case ERR_NONFINITE_RATIO: return "non-finite y/raw_mu ratio";
+        case ERR_NONFINITE_CORRECTION: return "non-finite multiplicative correction";
+        case ERR_NEGATIVE_CORRECTION: return "substantially negative multiplicative correction";
+        case ERR_NONFINITE_ESTIMATE: return "non-finite signed UPDC estimate";
+        case ERR_INVALID_NORM_WHT: return "invalid normalized WHT";
+        case ERR_NEGATIVE_YEFF: return "negative/non-finite y_eff reached solver";
+        case ERR_NONFINITE_INITIAL: return "non-finite signed initial estimate";
+        case ERR_INVALID_PSF_PIXEL: return "invalid PSF pixel";
+        case ERR_LINKMAP_TARGET: return "invalid or obsolete LinkMap cache";
+        default: return "unknown device error";
+    }
+}
+
+int next_smooth(int n, bool even) {
+    for (;; ++n) {
+        if (even && (n & 1)) continue;
+        int q = n;
+        while (q % 2 == 0) q /= 2;
+        while (q % 3 == 0) q /= 3;
+        while (q % 5 == 0) q /= 5;
+        while (q % 7 == 0) q /= 7;
+        if (q == 1) return n;
+    }
+}
+
+bool fft_factor(int n, std::vector<int> &radices) {
+    radices.clear();
+    int m = n;
+    while (m % 8 == 0) { radices.push_back(8); m /= 8; }
+    while (m % 4 == 0) { radices.push_back(4); m /= 4; }
+    while (m % 2 == 0) { radices.push_back(2); m /= 2; }
+    for (int r : {7, 5, 3})
+        while (m % r == 0) { radices.push_back(r); m /= r; }
+    return m == 1 && (int)radices.size() <= FFT_MAX_STAGES;
+}
+
+template <typename T> std::vector<cx<T>> fft_make_table(int n, FftPlan &plan) {
+    std::vector<int> rad;
+    if (!fft_factor(n, rad)) throw Error(1, "FFT length " + std::to_string(n) + " is not 7-smooth");
+    std::vector<cx<T>> tab;
+    plan.n = n;
+    plan.nstage = (int)rad.size();
+    int ns = 1;
+    const double two_pi = 6.283185307179586476925286766559;
+    for (size_t s = 0; s < rad.size(); ++s) {
+        const int R = rad[s];
+        plan.radix[s] = R;
+        plan.ns[s] = ns;
+        plan.twoff[s] = (int)tab.size();
+        for (int k = 0; k < ns; ++k)
+            for (int r = 1; r < R; ++r) {
+                const double a = -two_pi * (double)r * (double)k / ((double)ns * (double)R);
+                tab.push_back(cx<T>{(T)std::cos(a), (T)std::sin(a)});
+            }
+        ns *= R;
+    }
+    if (tab.empty()) tab.push_back(cx<T>{1, 0});
+    return tab;
+}
+template std::vector<cx<float>> fft_make_table<float>(int, FftPlan &);
+template std::vector<cx<double>> fft_make_table<double>(int, FftPlan &);
+
+namespace {
+
+constexpr int NT = 512;
+constexpr size_t SMEM_LIMIT = 227 * 1024;
+
+template <typename T> struct Caps;
+template <> struct Caps<float> {
+    static constexpr int ROW = 11264;
+    static constexpr int COL_S = 5632;
+    static constexpr int COL_L = 11264;
+};
+template <> struct Caps<double> {
+    static constexpr int ROW = 5632;
+    static constexpr int COL_S = 5632;
+    static constexpr int COL_L = 11264;
+};
+
+template <typename T> T *dalloc(size_t n, size_t *counter) {
+    T *p = nullptr;
+    UPDC_CUDA(cudaMalloc(&p, (n ? n : 1) * sizeof(T)));
+    if (counter) *counter += (n ? n : 1) * sizeof(T);
+    return p;
+}
+
+int grid1d(size_t n, int threads = 256) {
+    size_t g = (n + threads - 1) / threads;
+    if (g > 148 * 16) g = 148 * 16;
+    return (int)(g ? g : 1);
+}
+
+template <typename K> void set_smem(K kern, size_t bytes) {
+    UPDC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+bool read_f32_exact(const std::string &path, float *out, size_t count) {
+    FILE *f = fopen(path.c_str(), "rb");
+    if (!f) return false;
+    const bool ok = fread(out, sizeof(float), count, f) == count && fgetc(f) == EOF;
+    fclose(f);
+    return ok;
+}
+
+// ---------------------------------------------------------------------------- engine
+template <typename T> class EngineImpl final : public Engine {
+  public:
+    explicit EngineImpl(const EngineOptions &o) : opt_(o) {
+        UPDC_CUDA(cudaSetDevice(opt_.device));
+        UPDC_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        comp_mu_ = opt_.compensated_mu >= 0 ? opt_.compensated_mu
+                                            : (opt_.form == FORM_FP32 || opt_.form == FORM_FP32_KAHAN ? 1 : 0);
+    }
+    ~EngineImpl() override {
+        if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+        if (graph_) cudaGraphDestroy(graph_);
+        for (auto &m : links_) m.release();
+        for (void *p : allocs_) cudaFree(p);
+        if (staging_) cudaFree(staging_);
+        if (pinned_) cudaFreeHost(pinned_);
+        for (auto e : events_) cudaEventDestroy(e);
+        if (stream_) cudaStreamDestroy(stream_);
+    }
+
+    // ------------------------------------------------------------------ load
+    void load(const std::string &manifest, int W, int H, int iw, int ih, int nexp, int transposed) override {
+        if (W < 1 || H < 1 || iw < 1 || ih < 1 || nexp < 1) throw Error(1, "invalid dimensions/exposures/iterations/workers/save_every");
+        W_ = W; H_ = H; iw_ = iw; ih_ = ih; nexp_ = nexp; transposed_ = transposed ? 1 : 0;
+        nout_ = (size_t)W * H;
+        nin_ = (size_t)iw * ih;
+        if (nout_ > UINT32_MAX) throw Error(1, "target grid exceeds 32-bit link index capacity");
+        FILE *f = fopen(manifest.c_str(), "r");
+        if (!f) throw Error(1, "cannot open manifest");
+        exps_.assign(nexp, ExposureInput());
+        for (int k = 0; k < nexp; ++k) {
+            char line[8192];
+            if (!fgets(line, sizeof(line), f)) { fclose(f); throw Error(1, "manifest has fewer rows than expected"); }
+            char *save = nullptr, *fld[8];
+            for (int j = 0; j < 8; ++j) fld[j] = strtok_r(j ? nullptr : line, "\t\r\n", &save);
+            for (int j = 0; j < 8; ++j)
+                if (!fld[j]) { fclose(f); throw Error(1, "manifest requires science, weight, psf, psf_width, psf_height, vertices, background, pedestal"); }
+            ExposureInput &e = exps_[k];
+            e.science = fld[0]; e.weight = fld[1]; e.psf = fld[2];
+            e.psf_width = (int)strtol(fld[3], nullptr, 10);
+            e.psf_height = (int)strtol(fld[4], nullptr, 10);
+            e.vertices = fld[5];
+            e.links = e.vertices + ".links";
+            e.background = strtod(fld[6], nullptr);
+            e.pedestal = strtod(fld[7], nullptr);
+            e.backgroundf = strtof(fld[6], nullptr);
+            e.pedestalf = strtof(fld[7], nullptr);
+            if (e.psf_width < 1 || e.psf_height < 1) { fclose(f); throw Error(1, "invalid PSF dimensions in manifest"); }
+            const float mo = e.backgroundf + e.pedestalf;
+            if (!std::isfinite(e.backgroundf) || !std::isfinite(e.pedestalf) || e.pedestalf < 0.0f || !std::isfinite(mo)) {
+                fclose(f);
+                throw Error(1, "invalid background/pedestal in manifest");
+            }
+        }
+        char extra[8192];
+        const bool more = fgets(extra, sizeof(extra), f) != nullptr;
+        fclose(f);
+        if (more) throw Error(1, "manifest has more rows than expected");
+    }
+
+    // ------------------------------------------------------------------ setup
+    void setup() override {
+        const double t_all = now_s();
+        choose_fft_shape();
+        allocate();
+        double t0 = now_s();
+        for (int k = 0; k < nexp_; ++k) prepare_links(k);
+        setup_time_[0] = now_s() - t0;
+        t0 = now_s();
+        load_planes();
+        setup_time_[1] = now_s() - t0;
+        t0 = now_s();
+        prepare_psf_spectra();
+        setup_time_[2] = now_s() - t0;
+        t0 = now_s();
+        drizzle();
+        setup_time_[3] = now_s() - t0;
+        t0 = now_s();
+        denominator();
+        setup_time_[4] = now_s() - t0;
+        setup_time_[5] = now_s() - t_all;
+        setup_done_ = true;
+    }
+
+    void iterate(int n, bool check_each, std::vector<IterationRecord> *records) override {
+        if (!setup_done_) throw Error(1, "engine is not set up");
+        const bool graph = opt_.use_graph && !opt_.stage_timing;
+        if (graph && !graph_exec_) build_graph();
+        while ((int)events_.size() < 2 * (n + 1)) {
+            cudaEvent_t e;
+            UPDC_CUDA(cudaEventCreate(&e));
+            events_.push_back(e);
+        }
+        const size_t rec_bytes = rec_stride();
+        ensure_pinned((size_t)n * rec_bytes);
+        int done = 0;
+        while (done < n) {
+            const int batch = check_each ? 1 : n - done;
+            for (int i = 0; i < batch; ++i) {
+                UPDC_CUDA(cudaEventRecord(events_[2 * (done + i)], stream_));
+                if (graph) UPDC_CUDA(cudaGraphLaunch(graph_exec_, stream_));
+                else enqueue_iteration(opt_.stage_timing != 0);
+                UPDC_CUDA(cudaEventRecord(events_[2 * (done + i) + 1], stream_));
+                char *dst = (char *)pinned_ + (size_t)(done + i) * rec_bytes;
+                UPDC_CUDA(cudaMemcpyAsync(dst, d_stats_, nexp_ * sizeof(ExpStats), cudaMemcpyDeviceToHost, stream_));
+                UPDC_CUDA(cudaMemcpyAsync(dst + nexp_ * sizeof(ExpStats), d_err_, 8, cudaMemcpyDeviceToHost, stream_));
+                UPDC_CUDA(cudaMemcpyAsync(dst + nexp_ * sizeof(ExpStats) + 8, d_red_sum_, 8, cudaMemcpyDeviceToHost, stream_));
+                UPDC_CUDA(cudaMemcpyAsync(dst + nexp_ * sizeof(ExpStats) + 16, d_red_neg_, 8, cudaMemcpyDeviceToHost, stream_));
+            }
+            UPDC_CUDA(cudaStreamSynchronize(stream_));
+            for (int i = 0; i < batch; ++i) {
+                const char *src = (const char *)pinned_ + (size_t)(done + i) * rec_bytes;
+                unsigned long long key;
+                memcpy(&key, src + nexp_ * sizeof(ExpStats), 8);
+                if (key != ~0ull) raise_device_error(key);
+                if (records) {
+                    IterationRecord r;
+                    float ms = 0;
+                    UPDC_CUDA(cudaEventElapsedTime(&ms, events_[2 * (done + i)], events_[2 * (done + i) + 1]));
+                    r.seconds = ms * 1e-3;
+                    if (opt_.stage_timing)
+                        for (int s = 0; s < 8; ++s) r.stage_seconds[s] = stage_ms_[s] * 1e-3;
+                    const ExpStats *st = (const ExpStats *)src;
+                    for (int k = 0; k < nexp_; ++k) {
+                        r.new_frozen.push_back(st[k].nnew);
+                        r.total_frozen.push_back(st[k].ntotal);
+                        r.min_raw_mu.push_back(st[k].min_ordered == ~0ull ? INFINITY : ordered_to_double(st[k].min_ordered));
+                    }
+                    memcpy(&r.signed_sum, src + nexp_ * sizeof(ExpStats) + 8, 8);
+                    memcpy(&r.negative, src + nexp_ * sizeof(ExpStats) + 16, 8);
+                    records->push_back(std::move(r));
+                }
+            }
+            done += batch;
+        }
+    }
+
+    // ------------------------------------------------------------------ planes
+    // Host <-> device plane copies on the engine's stream.  When the host type
+    // is the engine's type the copy is direct (pinned host memory gives full
+    // PCIe/C2C bandwidth); otherwise the raw host data goes through a device
+    // staging buffer and is converted by a kernel.
+    void read_plane(int which, int k, void *host, int as_double) override {
+        size_t n;
+        const void *src = plane_ptr(which, k, &n);
+        if (which == PLANE_FROZEN) {
+            UPDC_CUDA(cudaMemcpyAsync(host, src, n, cudaMemcpyDeviceToHost, stream_));
+        } else if ((as_double != 0) == (sizeof(T) == 8)) {
+            UPDC_CUDA(cudaMemcpyAsync(host, src, n * sizeof(T), cudaMemcpyDeviceToHost, stream_));
+        } else {
+            void *st = staging(n * 8);
+            if (as_double) k_convert<T, double><<<grid1d(n), 256, 0, stream_>>>((const T *)src, (double *)st, n);
+            else k_convert<T, float><<<grid1d(n), 256, 0, stream_>>>((const T *)src, (float *)st, n);
+            UPDC_CUDA(cudaGetLastError());
+            UPDC_CUDA(cudaMemcpyAsync(host, st, n * (as_double ? 8 : 4), cudaMemcpyDeviceToHost, stream_));
+        }
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+    }
+    void write_plane(int which, int k, const void *host, int as_double) override {
+        size_t n;
+        void *dst = const_cast<void *>(plane_ptr(which, k, &n));
+        if (which == PLANE_FROZEN) {
+            UPDC_CUDA(cudaMemcpyAsync(dst, host, n, cudaMemcpyHostToDevice, stream_));
+        } else if ((as_double != 0) == (sizeof(T) == 8)) {
+            UPDC_CUDA(cudaMemcpyAsync(dst, host, n * sizeof(T), cudaMemcpyHostToDevice, stream_));
+        } else {
+            void *st = staging(n * 8);
+            UPDC_CUDA(cudaMemcpyAsync(st, host, n * (as_double ? 8 : 4), cudaMemcpyHostToDevice, stream_));
+            if (as_double) k_convert<double, T><<<grid1d(n), 256, 0, stream_>>>((const double *)st, (T *)dst, n);
+            else k_convert<float, T><<<grid1d(n), 256, 0, stream_>>>((const float *)st, (T *)dst, n);
+            UPDC_CUDA(cudaGetLastError());
+        }
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+    }
+    void *staging(size_t bytes) {
+        if (bytes > staging_bytes_) {
+            if (staging_) cudaFree(staging_);
+            staging_ = nullptr;
+            UPDC_CUDA(cudaMalloc(&staging_, bytes));
+            staging_bytes_ = bytes;
+        }
+        return staging_;
+    }
+    void *staging_ = nullptr;
+    size_t staging_bytes_ = 0;
+
+    void stage_forward(int k) override {
+        (void)k;
+        reset_iteration_state();
+        launch_row_r2c_plane(estimate_, rx_, 1, 0, 0);
+        launch_col_forward();
+        launch_row_c2r_batched(y_, nexp_, blur_);
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+    }
+    void stage_detector(int k, IterationRecord *rec) override {
+        reset_iteration_state();
+        launch_detector();
+        launch_scatter(wr_, scatter_);
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+        check_error();
+        if (rec) {
+            std::vector<ExpStats> st(nexp_);
+            UPDC_CUDA(cudaMemcpy(st.data(), d_stats_, nexp_ * sizeof(ExpStats), cudaMemcpyDeviceToHost));
+            rec->new_frozen.clear(); rec->total_frozen.clear(); rec->min_raw_mu.clear();
+            for (int j = 0; j < nexp_; ++j) {
+                rec->new_frozen.push_back(st[j].nnew);
+                rec->total_frozen.push_back(st[j].ntotal);
+                rec->min_raw_mu.push_back(st[j].min_ordered == ~0ull ? INFINITY : ordered_to_double(st[j].min_ordered));
+            }
+        }
+        (void)k;
+    }
+    void stage_correction() override {
+        launch_row_r2c_plane(scatter_, rs_, nexp_, nout_, (size_t)(M_ + 1) * H_);
+        launch_col_adjoint();
+        launch_row_c2r_batched(cr_, 1, correction_);
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+    }
+    void stage_update(IterationRecord *rec) override {
+        reset_iteration_state();
+        launch_update();
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+        check_error();
+        if (rec) {
+            UPDC_CUDA(cudaMemcpy(&rec->signed_sum, d_red_sum_, 8, cudaMemcpyDeviceToHost));
+            UPDC_CUDA(cudaMemcpy(&rec->negative, d_red_neg_, 8, cudaMemcpyDeviceToHost));
+        }
+    }
+    void decode_links(int k, uint32_t *host_targets) override {
+        const DevLinkMap &m = links_.at(k);
+        uint32_t *d = dalloc<uint32_t>(m.nlinks, nullptr);
+        linkmap_decode(m, d, stream_);
+        UPDC_CUDA(cudaMemcpyAsync(host_targets, d, m.nlinks * 4, cudaMemcpyDeviceToHost, stream_));
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+        cudaFree(d);
+    }
+    uint64_t link_count(int k) const override { return links_.at(k).nlinks; }
+    int link_encoding(int k) const override { return (int)links_.at(k).encoding; }
+    double scalar(int which) const override {
+        switch (which) {
+            case 0: return (double)weight_scale_;
+            case 1: return (double)max_sens_;
+            case 2: return FW_;
+            case 3: return FH_;
+            case 4: return (double)masked_;
+            case 5: return sizeof(T) * 8;
+            case 6: return comp_mu_;
+            default: return 0;
+        }
+    }
+    size_t device_bytes() const override { return bytes_; }
+    const std::vector<ExposureInput> &exposures() const override { return exps_; }
+    double setup_seconds(int stage) const override { return stage >= 0 && stage < 8 ? setup_time_[stage] : 0; }
+    void set_stage_timing(int on) override { opt_.stage_timing = on ? 1 : 0; }
+
+  private:
+    EngineOptions opt_;
+    cudaStream_t stream_ = nullptr;
+    int comp_mu_ = 0;
+    int W_ = 0, H_ = 0, iw_ = 0, ih_ = 0, nexp_ = 0, transposed_ = 0, FW_ = 0, FH_ = 0, M_ = 0;
+    size_t nout_ = 0, nin_ = 0, bytes_ = 0;
+    std::vector<ExposureInput> exps_;
+    std::vector<DevLinkMap> links_;
+    std::vector<void *> allocs_;
+    bool setup_done_ = false;
+    double setup_time_[8] = {};
+    float stage_ms_[8] = {};
+
+    FftPlan plan_m_, plan_h_;
+    const FftPlan *d_plan_m_ = nullptr, *d_plan_h_ = nullptr;
+    cx<T> *post_ = nullptr;
+    T *estimate_ = nullptr, *coverage_ = nullptr, *den_ = nullptr, *correction_ = nullptr;
+    T *blur_ = nullptr, *wr_ = nullptr, *scatter_ = nullptr, *sci_ = nullptr, *wht_ = nullptr;
+    uint8_t *frozen_ = nullptr;
+    cx<T> *rx_ = nullptr, *y_ = nullptr, *rs_ = nullptr, *cr_ = nullptr, *khat_ = nullptr;
+    cx<T> *aux_fwd_ = nullptr;
+    void *aux_adj_ = nullptr;
+    ExpDesc<T> *d_exps_ = nullptr;
+    ExpStats *d_stats_ = nullptr;
+    unsigned long long *d_err_ = nullptr, *d_red_neg_ = nullptr, *d_part_neg_ = nullptr;
+    double *d_part_sum_ = nullptr, *d_red_sum_ = nullptr;
+    int upd_grid_ = 0;
+    T weight_scale_ = 0, max_sens_ = 0;
+    uint64_t masked_ = 0;
+    void *pinned_ = nullptr;
+    size_t pinned_bytes_ = 0;
+    std::vector<cudaEvent_t> events_;
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t graph_exec_ = nullptr;
+
+    template <typename U> U *alloc(size_t n) {
+        U *p = dalloc<U>(n, &bytes_);
+        allocs_.push_back(p);
+        return p;
+    }
+    size_t rec_stride() const { return align16(nexp_ * sizeof(ExpStats) + 24); }
+    void ensure_pinned(size_t bytes) {
+        if (bytes <= pinned_bytes_) return;
+        if (pinned_) cudaFreeHost(pinned_);
+        UPDC_CUDA(cudaMallocHost(&pinned_, bytes));
+        pinned_bytes_ = bytes;
+    }
+
+    const FftPlan *upload_plan(const FftPlan &p) {
+        FftPlan *d = alloc<FftPlan>(1);
+        UPDC_CUDA(cudaMemcpy(d, &p, sizeof(FftPlan), cudaMemcpyHostToDevice));
+        return d;
+    }
+
+    bool acc_fp64() const { return opt_.form == FORM_FP32 && sizeof(T) == 4; }
+
+    void choose_fft_shape() {
+        int mpw = 0, mph = 0;
+        for (auto &e : exps_) {
+            mpw = std::max(mpw, e.psf_width);
+            mph = std::max(mph, e.psf_height);
+        }
+        const int pad_w = transposed_ ? mph : mpw, pad_h = transposed_ ? mpw : mph;
+        const int min_w = W_ + pad_w - 1, min_h = H_ + pad_h - 1;
+        FW_ = opt_.fft_width ? opt_.fft_width : next_smooth(min_w, true);
+        FH_ = opt_.fft_height ? opt_.fft_height : next_smooth(min_h, false);
+        if (FW_ < min_w || FH_ < min_h || (FW_ & 1)) throw Error(1, "FFT shape below the linear-convolution minimum or odd width");
+        M_ = FW_ / 2;
+        if (M_ > Caps<T>::ROW) throw Error(1, "FFT width exceeds the row-transform capacity");
+        if (FH_ > Caps<T>::COL_L) throw Error(1, "FFT height exceeds the column-transform capacity");
+        // twiddle tables
+        auto tm = fft_make_table<T>(M_, plan_m_);
+        auto th = fft_make_table<T>(FH_, plan_h_);
+        cx<T> *dm = alloc<cx<T>>(tm.size()), *dh = alloc<cx<T>>(th.size());
+        UPDC_CUDA(cudaMemcpy(dm, tm.data(), tm.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
+        UPDC_CUDA(cudaMemcpy(dh, th.data(), th.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
+        plan_m_.tw = dm;
+        plan_h_.tw = dh;
+        d_plan_m_ = upload_plan(plan_m_);
+        d_plan_h_ = upload_plan(plan_h_);
+        std::vector<cx<T>> post(M_ + 1);
+        const double two_pi = 6.283185307179586476925286766559;
+        for (int u = 0; u <= M_; ++u) post[u] = cx<T>{(T)std::cos(-two_pi * u / FW_), (T)std::sin(-two_pi * u / FW_)};
+        post_ = alloc<cx<T>>(M_ + 1);
+        UPDC_CUDA(cudaMemcpy(post_, post.data(), post.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
+    }
+
+    void allocate() {
+        const size_t nu = (size_t)M_ + 1;
+        estimate_ = alloc<T>(nout_);
+        coverage_ = alloc<T>(nout_);
+        den_ = alloc<T>(nout_);
+        correction_ = alloc<T>(nout_);
+        blur_ = alloc<T>(nexp_ * nout_);
+        scatter_ = alloc<T>(nexp_ * nout_);
+        wr_ = alloc<T>(nexp_ * nin_);
+        sci_ = alloc<T>(nexp_ * nin_);
+        wht_ = alloc<T>(nexp_ * nin_);
+        frozen_ = alloc<uint8_t>(nexp_ * nin_);
+        UPDC_CUDA(cudaMemset(frozen_, 0, nexp_ * nin_));
+        rx_ = alloc<cx<T>>(nu * H_);
+        cr_ = alloc<cx<T>>(nu * H_);
+        y_ = alloc<cx<T>>(nexp_ * nu * H_);
+        rs_ = alloc<cx<T>>(nexp_ * nu * H_);
+        khat_ = alloc<cx<T>>(nexp_ * nu * FH_);
+        d_exps_ = alloc<ExpDesc<T>>(nexp_);
+        d_stats_ = alloc<ExpStats>(nexp_);
+        d_err_ = alloc<unsigned long long>(1);
+        upd_grid_ = grid1d(nout_);
+        d_part_sum_ = alloc<double>(upd_grid_);
+        d_part_neg_ = alloc<unsigned long long>(upd_grid_);
+        d_red_sum_ = alloc<double>(1);
+        d_red_neg_ = alloc<unsigned long long>(1);
+        if (2 * align16((size_t)FH_ * sizeof(cx<T>)) > SMEM_LIMIT) aux_fwd_ = alloc<cx<T>>(nu * FH_);
+        links_.assign(nexp_, DevLinkMap());
+        // kernel attributes
+        configure_kernels();
+    }
+
+    // ------------------------------------------------------------------ kernel configuration
+    size_t row_smem() const { return (size_t)(Caps<T>::ROW / M_) * M_ * sizeof(cx<T>); }
+    int row_batch() const { return Caps<T>::ROW / M_; }
+    size_t fwd_smem() const { return aux_fwd_ ? align16(FH_ * sizeof(cx<T>)) : 2 * align16(FH_ * sizeof(cx<T>)); }
+    template <class Acc> size_t adj_smem() const {
+        const size_t b = align16(FH_ * sizeof(cx<T>)) + align16(FH_ * sizeof(typename Acc::S));
+        return b > SMEM_LIMIT ? align16(FH_ * sizeof(cx<T>)) : b;
+    }
+    template <class Acc> bool adj_aux() const {
+        return align16(FH_ * sizeof(cx<T>)) + align16(FH_ * sizeof(typename Acc::S)) > SMEM_LIMIT;
+    }
+
+    void configure_kernels() {
+        const size_t rs = row_smem();
+        set_smem(k_row_r2c<T, NT, Caps<T>::ROW, PlaneLoader<T>>, rs);
+        set_smem(k_row_r2c<T, NT, Caps<T>::ROW, PsfLoader<T>>, rs);
+        set_smem(k_row_c2r<T, NT, Caps<T>::ROW, PlaneStore<T>>, rs);
+        const size_t fs = fwd_smem();
+        set_smem(k_col_forward<T, NT, Caps<T>::COL_S>, fs);
+        set_smem(k_col_forward<T, NT, Caps<T>::COL_L>, fs);
+        set_smem(k_col_fft<T, NT, Caps<T>::COL_S, false>, align16(FH_ * sizeof(cx<T>)));
+        set_smem(k_col_fft<T, NT, Caps<T>::COL_L, false>, align16(FH_ * sizeof(cx<T>)));
+        configure_adjoint<AccPlain<T>>();
+        if (sizeof(T) == 4) {
+            configure_adjoint<AccF64>();
+            configure_adjoint<AccKahan>();
+        }
+    }
+    template <class Acc> void configure_adjoint() {
+        if constexpr (sizeof(typename Acc::S) > 0) {
+            if constexpr (std::is_same<Acc, AccPlain<T>>::value || sizeof(T) == 4) {
+                const size_t s = adj_smem<Acc>();
+                set_smem(k_col_adjoint<T, Acc, NT, Caps<T>::COL_S>, s);
+                set_smem(k_col_adjoint<T, Acc, NT, Caps<T>::COL_L>, s);
+            }
+        }
+    }
+
+    // ------------------------------------------------------------------ launches
+    template <class Loader>
+    void launch_row_r2c(const Loader &ld, int rows, int batch, cx<T> *out, int ldo, size_t out_stride) {
+        const int B = row_batch();
+        dim3 grid((unsigned)ceil_div(rows, B), (unsigned)batch);
+        k_row_r2c<T, NT, Caps<T>::ROW, Loader><<<grid, NT, row_smem(), stream_>>>(d_plan_m_, post_, ld, W_, rows, B, out, ldo, out_stride);
+        UPDC_CUDA(cudaGetLastError());
+    }
+    // planes [batch][H][W] -> u-major [batch][M+1][H]
+    void launch_row_r2c_plane(const T *plane, cx<T> *out, int batch, size_t plane_stride, size_t out_stride) {
+        if (batch == 1) {
+            launch_row_r2c(PlaneLoader<T>{plane, W_}, H_, 1, out, H_, 0);
+            return;
+        }
+        for (int k = 0; k < batch; ++k)
+            launch_row_r2c(PlaneLoader<T>{plane + k * plane_stride, W_}, H_, 1, out + k * out_stride, H_, 0);
+    }
+    void launch_col_forward() {
+        const size_t nu = (size_t)M_ + 1;
+        const size_t ks = nu * FH_, ys = nu * H_;
+        if (FH_ <= Caps<T>::COL_S)
+            k_col_forward<T, NT, Caps<T>::COL_S><<<(unsigned)nu, NT, fwd_smem(), stream_>>>(d_plan_h_, rx_, H_, H_, khat_, ks, nexp_, y_, H_, ys, H_, (int)nu, aux_fwd_);
+        else
+            k_col_forward<T, NT, Caps<T>::COL_L><<<(unsigned)nu, NT, fwd_smem(), stream_>>>(d_plan_h_, rx_, H_, H_, khat_, ks, nexp_, y_, H_, ys, H_, (int)nu, aux_fwd_);
+        UPDC_CUDA(cudaGetLastError());
+    }
+    template <class Acc> void launch_col_adjoint_t(const cx<T> *khat) {
+        const size_t nu = (size_t)M_ + 1;
+        typename Acc::S *aux = nullptr;
+        if (adj_aux<Acc>()) {
+            if (!aux_adj_) aux_adj_ = alloc<typename Acc::S>(nu * FH_);
+            aux = (typename Acc::S *)aux_adj_;
+        }
+        const size_t s = adj_smem<Acc>();
+        if (FH_ <= Caps<T>::COL_S)
+            k_col_adjoint<T, Acc, NT, Caps<T>::COL_S><<<(unsigned)nu, NT, s, stream_>>>(d_plan_h_, rs_, H_, nu * H_, H_, khat, nu * FH_, nexp_, cr_, H_, H_, aux);
+        else
+            k_col_adjoint<T, Acc, NT, Caps<T>::COL_L><<<(unsigned)nu, NT, s, stream_>>>(d_plan_h_, rs_, H_, nu * H_, H_, khat, nu * FH_, nexp_, cr_, H_, H_, aux);
+        UPDC_CUDA(cudaGetLastError());
+    }
+    void launch_col_adjoint() {
+        if constexpr (sizeof(T) == 4) {
+            if (opt_.form == FORM_FP32) return launch_col_adjoint_t<AccF64>(khat_);
+            if (opt_.form == FORM_FP32_KAHAN) return launch_col_adjoint_t<AccKahan>(khat_);
+        }
+        launch_col_adjoint_t<AccPlain<T>>(khat_);
+    }
+    void launch_row_c2r_batched(const cx<T> *in, int batch, T *out) {
+        const int B = row_batch();
+        dim3 grid((unsigned)ceil_div(H_, B), (unsigned)batch);
+        const T scale = scale_factor();
+        k_row_c2r<T, NT, Caps<T>::ROW, PlaneStore<T>><<<grid, NT, row_smem(), stream_>>>(
+            d_plan_m_, post_, in, H_, (size_t)(M_ + 1) * H_, H_, W_, B, scale, PlaneStore<T>{out, W_, nout_});
+        UPDC_CUDA(cudaGetLastError());
+    }
+    T scale_factor() const {
+        // updc_core.c:741 scale = 1.0f/(float)nf
+        if (sizeof(T) == 4) return (T)(1.0f / (float)((size_t)FW_ * FH_));
+        return (T)(1.0 / (double)((size_t)FW_ * FH_));
+    }
+    void launch_detector() {
+        dim3 grid((unsigned)std::min<size_t>(ceil_div(nin_, 256), 148 * 8), (unsigned)nexp_);
+        if (comp_mu_) k_detector<T, true><<<grid, 256, 0, stream_>>>(d_exps_, nin_, nout_, blur_, wr_, d_stats_, d_err_);
+        else k_detector<T, false><<<grid, 256, 0, stream_>>>(d_exps_, nin_, nout_, blur_, wr_, d_stats_, d_err_);
+        UPDC_CUDA(cudaGetLastError());
+    }
+    void launch_scatter(const T *vals, T *out) {
+        dim3 grid((unsigned)std::min<size_t>(ceil_div(nout_, 256), 148 * 8), (unsigned)nexp_);
+        k_scatter_t<T, T, T><<<grid, 256, 0, stream_>>>(d_exps_, nin_, nout_, vals, 0, out);
+        UPDC_CUDA(cudaGetLastError());
+    }
+    void launch_update() {
+        k_update<T><<<upd_grid_, 256, 0, stream_>>>(nout_, correction_, den_, estimate_, max_sens_, d_err_, d_part_sum_, d_part_neg_);
+        k_reduce_partials<<<1, 256, 0, stream_>>>(d_part_sum_, d_part_neg_, upd_grid_, d_red_sum_, d_red_neg_);
+        UPDC_CUDA(cudaGetLastError());
+    }
+    void reset_iteration_state() {
+        // stats: nnew = ntotal = 0, min = ~0
+        static_assert(sizeof(ExpStats) == 32, "ExpStats layout");
+        std::vector<ExpStats> init(nexp_);
+        for (auto &s : init) { s.nnew = 0; s.ntotal = 0; s.min_ordered = ~0ull; s.pad = 0; }
+        if (!stats_init_) {
+            stats_init_ = alloc<ExpStats>(nexp_);
+            UPDC_CUDA(cudaMemcpy(stats_init_, init.data(), nexp_ * sizeof(ExpStats), cudaMemcpyHostToDevice));
+        }
+        UPDC_CUDA(cudaMemcpyAsync(d_stats_, stats_init_, nexp_ * sizeof(ExpStats), cudaMemcpyDeviceToDevice, stream_));
+        UPDC_CUDA(cudaMemsetAsync(d_err_, 0xFF, 8, stream_));
+    }
+    ExpStats *stats_init_ = nullptr;
+
+    void enqueue_iteration(bool timed) {
+        cudaEvent_t ev[9];
+        if (timed) {
+            for (auto &e : ev) UPDC_CUDA(cudaEventCreate(&e));
+            UPDC_CUDA(cudaEventRecord(ev[0], stream_));
+        }
+        reset_iteration_state();
+        launch_row_r2c_plane(estimate_, rx_, 1, 0, 0);                      // estimate R2C, x pass
+        if (timed) UPDC_CUDA(cudaEventRecord(ev[1], stream_));
+        launch_col_forward();                                               // y pass + OTF + inverse y pass
+        if (timed) UPDC_CUDA(cudaEventRecord(ev[2], stream_));
+        launch_row_c2r_batched(y_, nexp_, blur_);                           // inverse x pass + crop
+        if (timed) UPDC_CUDA(cudaEventRecord(ev[3], stream_));
+        launch_detector();                                                  // gather / FreezeMu / ratio
+        if (timed) UPDC_CUDA(cudaEventRecord(ev[4], stream_));
+        launch_scatter(wr_, scatter_);                                      // S^T (transposed gather)
+        if (timed) UPDC_CUDA(cudaEventRecord(ev[5], stream_));
+        launch_row_r2c_plane(scatter_, rs_, nexp_, nout_, (size_t)(M_ + 1) * H_);  // scatter R2C, x pass
+        if (timed) UPDC_CUDA(cudaEventRecord(ev[6], stream_));
+        launch_col_adjoint();                                               // y pass, conj-OTF sum, inverse y
+        launch_row_c2r_batched(cr_, 1, correction_);                        // inverse x pass + crop
+        if (timed) UPDC_CUDA(cudaEventRecord(ev[7], stream_));
+        launch_update();
+        if (timed) {
+            UPDC_CUDA(cudaEventRecord(ev[8], stream_));
+            UPDC_CUDA(cudaEventSynchronize(ev[8]));
+            for (int s = 0; s < 8; ++s) UPDC_CUDA(cudaEventElapsedTime(&stage_ms_[s], ev[s], ev[s + 1]));
+            for (auto &e : ev) cudaEventDestroy(e);
+        }
+    }
+
+    void build_graph() {
+        // the stats-initialiser buffer must exist before capture
+        reset_iteration_state();
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+        UPDC_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        enqueue_iteration(false);
+        UPDC_CUDA(cudaStreamEndCapture(stream_, &graph_));
+        UPDC_CUDA(cudaGraphInstantiate(&graph_exec_, graph_, 0));
+    }
+
+    [[noreturn]] void raise_device_error(unsigned long long key) {
+        const uint32_t code = (uint32_t)(key & 0xFF);
+        const uint64_t index = (key >> 8) & 0xFFFFFFFFFFull;
+        std::string detail;
+        if (code == ERR_NEGATIVE_CORRECTION && index < nout_) {
+            T c = 0, d = 0;
+            UPDC_CUDA(cudaMemcpy(&c, correction_ + index, sizeof(T), cudaMemcpyDeviceToHost));
+            UPDC_CUDA(cudaMemcpy(&d, den_ + index, sizeof(T), cudaMemcpyDeviceToHost));
+            char buf[256];
+            snprintf(buf, sizeof(buf), "negative correction at target %llu: C=%.9g numerator=%.9g denominator=%.9g\n",
+                     (unsigned long long)index, (double)(c / d), (double)c, (double)d);
+            fputs(buf, stderr);
+        }
+        throw Error(1, error_message(code));
+    }
+    void check_error() {
+        unsigned long long key;
+        UPDC_CUDA(cudaMemcpy(&key, d_err_, 8, cudaMemcpyDeviceToHost));
+        if (key != ~0ull) raise_device_error(key);
+    }
+
+    const void *plane_ptr(int which, int k, size_t *n) {
+        *n = nout_;
+        switch (which) {
+            case PLANE_ESTIMATE: return estimate_;
+            case PLANE_COVERAGE: return coverage_;
+            case PLANE_DENOMINATOR: return den_;
+            case PLANE_CORRECTION: return correction_;
+            case PLANE_BLUR: return blur_ + (size_t)k * nout_;
+            case PLANE_SCATTER: return scatter_ + (size_t)k * nout_;
+            case PLANE_SCIENCE: *n = nin_; return sci_ + (size_t)k * nin_;
+            case PLANE_WEIGHT: *n = nin_; return wht_ + (size_t)k * nin_;
+            case PLANE_WR: *n = nin_; return wr_ + (size_t)k * nin_;
+            case PLANE_FROZEN: *n = nin_; return frozen_ + (size_t)k * nin_;
+            default: throw Error(1, "unknown plane");
+        }
+    }
+
+    // ------------------------------------------------------------------ setup stages
+    void prepare_links(int k) {
+        ExposureInput &e = exps_[k];
+        DevLinkMap &m = links_[k];
+        bool ok = opt_.reuse_links && linkmap_load(e.links, nin_, W_, H_, m, stream_);
+        if (!ok) {
+            LinkBuildStats st;
+            linkmap_build(e.vertices, e.links, iw_, ih_, W_, H_, stream_, &st);
+            if (opt_.verbose)
+                printf("AreaLink exposure %d: %llu overlaps; encoding=%s; active=%llu, max-links=%u (GPU)\n", k + 1,
+                       (unsigned long long)st.nlinks, st.encoding == LINKMAP_DELTA16 ? "DELTA16" : "ABS32",
+                       (unsigned long long)st.active, st.max_links);
+            if (!linkmap_load(e.links, nin_, W_, H_, m, stream_)) throw Error(1, "invalid or obsolete LinkMap cache");
+        } else if (opt_.verbose) {
+            printf("AreaLink exposure %d: persistent cache hit (%s)\n", k + 1,
+                   m.encoding == LINKMAP_DELTA16 ? "DELTA16" : "ABS32");
+        }
+        linkmap_transpose(m, nout_, stream_);
+        bytes_ += m.file_bytes - 64 + (nout_ + 1) * 4 + m.nlinks * 8;
+    }
+
+    void upload_descs() {
+        std::vector<ExpDesc<T>> h(nexp_);
+        for (int k = 0; k < nexp_; ++k) {
+            const DevLinkMap &m = links_[k];
+            ExpDesc<T> &d = h[k];
+            d.off = m.off; d.base = m.base; d.tgt = m.tgt; d.delta = m.delta; d.frac = m.frac;
+            d.toff = m.toff; d.tsrc = m.tsrc; d.tfrac = m.tfrac;
+            d.sci = sci_ + (size_t)k * nin_;
+            d.wht = wht_ + (size_t)k * nin_;
+            d.frozen = frozen_ + (size_t)k * nin_;
+            const ExposureInput &e = exps_[k];
+            if (sizeof(T) == 4) {
+                d.background = (T)e.backgroundf;
+                d.pedestal = (T)e.pedestalf;
+                d.mean_offset = (T)(e.backgroundf + e.pedestalf);
+            } else {
+                d.background = (T)e.background;
+                d.pedestal = (T)e.pedestal;
+                d.mean_offset = (T)(e.background + e.pedestal);
+            }
+            d.delta16 = m.encoding == LINKMAP_DELTA16;
+        }
+        UPDC_CUDA(cudaMemcpy(d_exps_, h.data(), nexp_ * sizeof(ExpDesc<T>), cudaMemcpyHostToDevice));
+    }
+
+    void load_planes() {
+        float *h = nullptr;
+        UPDC_CUDA(cudaMallocHost(&h, 2 * nin_ * sizeof(float)));
+        float *d_raw = dalloc<float>(2 * nin_ * nexp_, nullptr);
+        // every 64th weight of every exposure, finite and > 0 (updc_core.c:379-386)
+        float *d_sample = dalloc<float>(nexp_ * (nin_ / 64 + 1) + 1, nullptr);
+        unsigned int *d_count = dalloc<unsigned int>(1, nullptr);
+        UPDC_CUDA(cudaMemset(d_count, 0, 4));
+        for (int k = 0; k < nexp_; ++k) {
+            if (!read_f32_exact(exps_[k].science, h, nin_)) { cudaFreeHost(h); throw Error(1, "cannot read SCI raw: " + exps_[k].science); }
+            if (!read_f32_exact(exps_[k].weight, h + nin_, nin_)) { cudaFreeHost(h); throw Error(1, "cannot read WHT raw: " + exps_[k].weight); }
+            UPDC_CUDA(cudaMemcpy(d_raw + 2 * nin_ * k, h, 2 * nin_ * sizeof(float), cudaMemcpyHostToDevice));
+            k_weight_sample<<<grid1d(nin_ / 64 + 1), 256, 0, stream_>>>(nin_, d_raw + 2 * nin_ * k + nin_, d_sample, d_count);
+        }
+        unsigned int n = 0;
+        UPDC_CUDA(cudaMemcpyAsync(&n, d_count, 4, cudaMemcpyDeviceToHost, stream_));
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+        cudaFreeHost(h);
+        if (!n) throw Error(1, "all input WHT pixels are zero");
+        // median sample[n/2] of the sorted samples (positive floats sort as their bits)
+        float *d_sorted = dalloc<float>(n, nullptr);
+        size_t tmp_bytes = 0;
+        cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, (const uint32_t *)d_sample, (uint32_t *)d_sorted, (int)n, 0, 32, stream_);
+        void *tmp = dalloc<char>(tmp_bytes, nullptr);
+        cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, (const uint32_t *)d_sample, (uint32_t *)d_sorted, (int)n, 0, 32, stream_);
+        float scale = 0;
+        UPDC_CUDA(cudaMemcpyAsync(&scale, d_sorted + n / 2, 4, cudaMemcpyDeviceToHost, stream_));
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+        cudaFree(tmp);
+        cudaFree(d_sorted);
+        cudaFree(d_sample);
+        if (!(scale > 0) || !std::isfinite(scale)) { cudaFree(d_raw); cudaFree(d_count); throw Error(1, "invalid WHT normalization"); }
+        weight_scale_ = (T)scale;
+        unsigned long long *d_masked = dalloc<unsigned long long>(1, nullptr);
+        UPDC_CUDA(cudaMemset(d_masked, 0, 8));
+        UPDC_CUDA(cudaMemset(d_err_, 0xFF, 8));
+        for (int k = 0; k < nexp_; ++k) {
+            const T ped = sizeof(T) == 4 ? (T)exps_[k].pedestalf : (T)exps_[k].pedestal;
+            k_weight_norm<T><<<grid1d(nin_), 256, 0, stream_>>>(nin_, d_raw + 2 * nin_ * k, d_raw + 2 * nin_ * k + nin_,
+                                                                 sci_ + (size_t)k * nin_, wht_ + (size_t)k * nin_,
+                                                                 weight_scale_, ped, k, d_masked, d_err_);
+        }
+        UPDC_CUDA(cudaGetLastError());
+        unsigned long long hm = 0;
+        UPDC_CUDA(cudaMemcpyAsync(&hm, d_masked, 8, cudaMemcpyDeviceToHost, stream_));
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+        masked_ = hm;
+        cudaFree(d_masked);
+        cudaFree(d_raw);
+        cudaFree(d_count);
+        check_error();
+        upload_descs();
+    }
+
+    // PSF spectra K_k (u-major, (M+1) x FH) of precision U into dst.
+    template <typename U> void psf_spectra(cx<U> *dst, bool fp64_sum, const FftPlan *pm, const FftPlan *ph, const cx<U> *post) {
+        const size_t nu = (size_t)M_ + 1;
+        cx<U> *rp = dalloc<cx<U>>(nu * FH_, nullptr);
+        for (int k = 0; k < nexp_; ++k) {
+            const ExposureInput &e = exps_[k];
+            const size_t count = (size_t)e.psf_width * e.psf_height;
+            std::vector<float> hp(count);
+            if (!read_f32_exact(e.psf, hp.data(), count)) { cudaFree(rp); throw Error(1, "cannot read PSF raw: " + e.psf); }
+            float *dp = dalloc<float>(count, nullptr);
+            UPDC_CUDA(cudaMemcpy(dp, hp.data(), count * 4, cudaMemcpyHostToDevice));
+            UPDC_CUDA(cudaMemset(d_err_, 0xFF, 8));
+            double sum = 0;
+            if (fp64_sum) {
+                const int g = 148;
+                double *part = dalloc<double>(g, nullptr);
+                k_psf_sum_f64<<<g, 256, 0, stream_>>>(dp, count, part, d_err_);
+                std::vector<double> hpart(g);
+                UPDC_CUDA(cudaMemcpyAsync(hpart.data(), part, g * 8, cudaMemcpyDeviceToHost, stream_));
+                UPDC_CUDA(cudaStreamSynchronize(stream_));
+                for (double v : hpart) sum += v;
+                cudaFree(part);
+            } else {
+                float *ds = dalloc<float>(1, nullptr);
+                k_psf_sum_neumaier<<<1, 1, 0, stream_>>>(dp, count, ds, d_err_);
+                float hs = 0;
+                UPDC_CUDA(cudaMemcpyAsync(&hs, ds, 4, cudaMemcpyDeviceToHost, stream_));
+                UPDC_CUDA(cudaStreamSynchronize(stream_));
+                sum = hs;
+                cudaFree(ds);
+            }
+            check_error();
+            if (!(sum > 0) || !std::isfinite(sum)) { cudaFree(dp); cudaFree(rp); throw Error(1, "PSF sum is zero/non-finite"); }
+            U inv;
+            if (fp64_sum) inv = (U)(1.0 / sum);
+            else inv = (U)(1.0f / (float)sum);
+            PsfLoader<U> ld{dp, e.psf_width, transposed_ ? e.psf_height : e.psf_width,
+                            transposed_ ? e.psf_width : e.psf_height, FW_, FH_, transposed_, inv};
+            const int B = Caps<U>::ROW / M_;
+            const size_t rsm = (size_t)B * M_ * sizeof(cx<U>);
+            set_smem(k_row_r2c<U, NT, Caps<U>::ROW, PsfLoader<U>>, rsm);
+            dim3 grid((unsigned)ceil_div(FH_, B), 1);
+            k_row_r2c<U, NT, Caps<U>::ROW, PsfLoader<U>><<<grid, NT, rsm, stream_>>>(pm, post, ld, FW_, FH_, B, rp, FH_, 0);
+            const size_t cs = align16(FH_ * sizeof(cx<U>));
+            cx<U> *out = dst + (size_t)k * nu * FH_;
+            if (FH_ <= Caps<U>::COL_S) {
+                set_smem(k_col_fft<U, NT, Caps<U>::COL_S, false>, cs);
+                k_col_fft<U, NT, Caps<U>::COL_S, false><<<(unsigned)nu, NT, cs, stream_>>>(ph, rp, FH_, FH_, out, FH_, FH_);
+            } else {
+                set_smem(k_col_fft<U, NT, Caps<U>::COL_L, false>, cs);
+                k_col_fft<U, NT, Caps<U>::COL_L, false><<<(unsigned)nu, NT, cs, stream_>>>(ph, rp, FH_, FH_, out, FH_, FH_);
+            }
+            UPDC_CUDA(cudaGetLastError());
+            UPDC_CUDA(cudaStreamSynchronize(stream_));
+            cudaFree(dp);
+        }
+        cudaFree(rp);
+    }
+
+    void prepare_psf_spectra() {
+        const bool fp64_sum = opt_.form == FORM_FP32 || opt_.form == FORM_FP64;
+        psf_spectra<T>(khat_, fp64_sum, d_plan_m_, d_plan_h_, post_);
+    }
+
+    void drizzle() {
+        UPDC_CUDA(cudaMemset(d_err_, 0xFF, 8));
+        k_drizzle<T><<<grid1d(nout_), 256, 0, stream_>>>(d_exps_, nexp_, nout_, estimate_, coverage_, d_err_);
+        UPDC_CUDA(cudaGetLastError());
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+        check_error();
+    }
+
+    // D = crop(C2R(sum_k conj(K_k) R2C(pad(S_k^T W_k)))) / nf   (updc_core.c:1026-1086)
+    void denominator() {
+        if (sizeof(T) == 4 && opt_.form == FORM_FP32) denominator_fp64();
+        else {
+            dim3 grid((unsigned)std::min<size_t>(ceil_div(nout_, 256), 148 * 8), (unsigned)nexp_);
+            k_scatter_t<T, T, T><<<grid, 256, 0, stream_>>>(d_exps_, nin_, nout_, (const T *)nullptr, 1, scatter_);
+            launch_row_r2c_plane(scatter_, rs_, nexp_, nout_, (size_t)(M_ + 1) * H_);
+            launch_col_adjoint();
+            launch_row_c2r_batched(cr_, 1, den_);
+        }
+        finish_denominator();
+    }
+
+    // FP32 form: the one-time denominator is computed entirely in FP64.
+    void denominator_fp64() {
+        using D = double;
+        const size_t nu = (size_t)M_ + 1;
+        FftPlan pm, ph;
+        auto tm = fft_make_table<D>(M_, pm);
+        auto th = fft_make_table<D>(FH_, ph);
+        cx<D> *dm = dalloc<cx<D>>(tm.size(), nullptr), *dh = dalloc<cx<D>>(th.size(), nullptr);
+        UPDC_CUDA(cudaMemcpy(dm, tm.data(), tm.size() * sizeof(cx<D>), cudaMemcpyHostToDevice));
+        UPDC_CUDA(cudaMemcpy(dh, th.data(), th.size() * sizeof(cx<D>), cudaMemcpyHostToDevice));
+        pm.tw = dm;
+        ph.tw = dh;
+        FftPlan *dpm = dalloc<FftPlan>(1, nullptr), *dph = dalloc<FftPlan>(1, nullptr);
+        UPDC_CUDA(cudaMemcpy(dpm, &pm, sizeof(FftPlan), cudaMemcpyHostToDevice));
+        UPDC_CUDA(cudaMemcpy(dph, &ph, sizeof(FftPlan), cudaMemcpyHostToDevice));
+        std::vector<cx<D>> post(M_ + 1);
+        const double two_pi = 6.283185307179586476925286766559;
+        for (int u = 0; u <= M_; ++u) post[u] = cx<D>{std::cos(-two_pi * u / FW_), std::sin(-two_pi * u / FW_)};
+        cx<D> *dpost = dalloc<cx<D>>(M_ + 1, nullptr);
+        UPDC_CUDA(cudaMemcpy(dpost, post.data(), post.size() * sizeof(cx<D>), cudaMemcpyHostToDevice));
+        cx<D> *kd = dalloc<cx<D>>(nexp_ * nu * FH_, nullptr);
+        psf_spectra<D>(kd, true, dpm, dph, dpost);
+        D *sc = dalloc<D>(nexp_ * nout_, nullptr);
+        dim3 grid((unsigned)std::min<size_t>(ceil_div(nout_, 256), 148 * 8), (unsigned)nexp_);
+        k_scatter_t<T, D, T><<<grid, 256, 0, stream_>>>(d_exps_, nin_, nout_, (const T *)nullptr, 1, sc);
+        cx<D> *rs = dalloc<cx<D>>(nexp_ * nu * H_, nullptr), *cr = dalloc<cx<D>>(nu * H_, nullptr);
+        const int B = Caps<D>::ROW / M_;
+        const size_t rsm = (size_t)B * M_ * sizeof(cx<D>);
+        set_smem(k_row_r2c<D, NT, Caps<D>::ROW, PlaneLoader<D>>, rsm);
+        for (int k = 0; k < nexp_; ++k) {
+            dim3 g((unsigned)ceil_div(H_, B), 1);
+            k_row_r2c<D, NT, Caps<D>::ROW, PlaneLoader<D>><<<g, NT, rsm, stream_>>>(dpm, dpost, PlaneLoader<D>{sc + k * nout_, W_}, W_, H_, B, rs + k * nu * H_, H_, 0);
+        }
+        const size_t b = align16(FH_ * sizeof(cx<D>));
+        const bool aux_needed = 2 * b > SMEM_LIMIT;
+        cx<D> *aux = aux_needed ? dalloc<cx<D>>(nu * FH_, nullptr) : nullptr;
+        const size_t s = aux_needed ? b : 2 * b;
+        if (FH_ <= Caps<D>::COL_S) {
+            set_smem(k_col_adjoint<D, AccPlain<D>, NT, Caps<D>::COL_S>, s);
+            k_col_adjoint<D, AccPlain<D>, NT, Caps<D>::COL_S><<<(unsigned)nu, NT, s, stream_>>>(dph, rs, H_, nu * H_, H_, kd, nu * FH_, nexp_, cr, H_, H_, aux);
+        } else {
+            set_smem(k_col_adjoint<D, AccPlain<D>, NT, Caps<D>::COL_L>, s);
+            k_col_adjoint<D, AccPlain<D>, NT, Caps<D>::COL_L><<<(unsigned)nu, NT, s, stream_>>>(dph, rs, H_, nu * H_, H_, kd, nu * FH_, nexp_, cr, H_, H_, aux);
+        }
+        D *den = dalloc<D>(nout_, nullptr);
+        set_smem(k_row_c2r<D, NT, Caps<D>::ROW, PlaneStore<D>>, rsm);
+        dim3 g2((unsigned)ceil_div(H_, B), 1);
+        k_row_c2r<D, NT, Caps<D>::ROW, PlaneStore<D>><<<g2, NT, rsm, stream_>>>(dpm, dpost, cr, H_, 0, H_, W_, B,
+                                                                                1.0 / (double)((size_t)FW_ * FH_), PlaneStore<D>{den, W_, 0});
+        k_convert<D, T><<<grid1d(nout_), 256, 0, stream_>>>(den, den_, nout_);
+        UPDC_CUDA(cudaGetLastError());
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+        for (void *p : {(void *)dm, (void *)dh, (void *)dpm, (void *)dph, (void *)dpost, (void *)kd, (void *)sc, (void *)rs, (void *)cr, (void *)aux, (void *)den})
+            if (p) cudaFree(p);
+    }
+
+    void finish_denominator() {
+        unsigned long long *d = dalloc<unsigned long long>(1, nullptr);
+        UPDC_CUDA(cudaMemset(d, 0, 8));
+        k_max_ordered<T><<<grid1d(nout_), 256, 0, stream_>>>(den_, nout_, d);
+        unsigned long long h = 0;
+        UPDC_CUDA(cudaMemcpyAsync(&h, d, 8, cudaMemcpyDeviceToHost, stream_));
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+        cudaFree(d);
+        double m = h ? ordered_to_double(h) : 0.0;
+        if (!(m > 0)) m = 0;  // the reference starts its maximum at 0
+        max_sens_ = (T)m;
+        if (!(max_sens_ > 0) || !std::isfinite((double)max_sens_)) throw Error(1, "invalid H^T W sensitivity");
+    }
+};
+
+}  // namespace
+
+std::unique_ptr<Engine> make_engine(const EngineOptions &opt) {
+    if (opt.form == FORM_FP64) return std::unique_ptr<Engine>(new EngineImpl<double>(opt));
+    return std::unique_ptr<Engine>(new EngineImpl<float>(opt));
+}
+
+}  // namespace updc

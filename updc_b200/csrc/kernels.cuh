@@ -1,0 +1,265 @@
+// Kernels of the UPDC iteration (sm_100a).  Spectra are stored "u-major":
+// for R2C along x (rows of FW reals -> M+1 = FW/2+1 bins) the bin u of every
+// row y is stored at spec[u * ld + y], so each u-row is one contiguous column
+// transform.  Only the first H (or rows_in) y-entries of a row-pass
+// intermediate are stored: the zero padding rows are never read or written.
+#pragma once
+
+#include "common.cuh"
+#include "fft.cuh"
+
+namespace updc {
+
+// ---------------------------------------------------------------------------- loaders
+template <typename T> struct PlaneLoader {
+    const T *p;
+    int pitch;
+    __device__ __forceinline__ T operator()(int y, int x) const { return p[(size_t)y * pitch + x]; }
+};
+
+// Centre-wrapped, normalised PSF on the FW x FH grid (updc_core.c:813-821):
+// PSF pixel (x, y) goes to ((x - fw/2) mod FW, (y - fh/2) mod FH); with
+// transposed storage the source index is x*pw + y.
+template <typename T> struct PsfLoader {
+    const float *psf;
+    int pw, fwid, fhei, FW, FH, transposed;
+    T inv;
+    __device__ __forceinline__ T operator()(int yy, int xx) const {
+        const int y = (yy + fhei / 2) % FH, x = (xx + fwid / 2) % FW;
+        if (y >= fhei || x >= fwid) return T(0);
+        const size_t src = transposed ? (size_t)x * pw + y : (size_t)y * pw + x;
+        return mul_rn((T)psf[src], inv);
+    }
+    __device__ __forceinline__ static float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+    __device__ __forceinline__ static double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+};
+
+// ---------------------------------------------------------------------------- row R2C
+// Rows [0, rows) of the real plane, zero-padded from W to FW = 2M columns,
+// transformed along x with an M-point complex FFT of z[m] = x[2m] + i x[2m+1]
+// and the split z -> X post-processing; bins are stored u-major.
+template <typename T, int NT, int CAP, class Loader>
+__global__ void __launch_bounds__(NT, 1) k_row_r2c(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ post, Loader ld, int W,
+                                                int rows, int B, cx<T> *__restrict__ out, int ldo, size_t out_batch_stride) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
+    const int M = plan->n;
+    const int y0 = blockIdx.x * B;
+    const int nb = min(B, rows - y0);
+    out += blockIdx.y * out_batch_stride;
+    for (int i = threadIdx.x; i < B * M; i += NT) {
+        const int b = i / M, m = i - b * M;
+        T a = 0, c = 0;
+        if (b < nb) {
+            const int x = 2 * m;
+            if (x < W) a = ld(y0 + b, x);
+            if (x + 1 < W) c = ld(y0 + b, x + 1);
+        }
+        buf[i] = {a, c};
+    }
+    __syncthreads();
+    fft_batch<false, NT, CAP>(buf, B, plan);
+    const T half = T(0.5);
+    for (int i = threadIdx.x; i < (M + 1) * B; i += NT) {
+        const int u = i / B, b = i - u * B;
+        if (b >= nb) continue;
+        const cx<T> *z = buf + b * M;
+        const cx<T> Z = z[u == M ? 0 : u];
+        const cx<T> Zm = z[u == 0 ? 0 : M - u];
+        const cx<T> Zc = {Zm.x, -Zm.y};
+        const cx<T> E = {half * (Z.x + Zc.x), half * (Z.y + Zc.y)};
+        const cx<T> D = {half * (Z.x - Zc.x), half * (Z.y - Zc.y)};
+        const cx<T> P = fmulc(D, post[u]);
+        out[(size_t)u * ldo + y0 + b] = {E.x + P.y, E.y - P.x};
+    }
+}
+
+// ---------------------------------------------------------------------------- row C2R
+__device__ __forceinline__ float mul_scale(float a, float s) { return __fmul_rn(a, s); }
+__device__ __forceinline__ double mul_scale(double a, double s) { return __dmul_rn(a, s); }
+template <typename T> struct PlaneStore {
+    T *p;
+    int pitch;
+    size_t batch_stride;
+    __device__ __forceinline__ void operator()(int k, int y, int x, T v) const { p[k * batch_stride + (size_t)y * pitch + x] = v; }
+};
+
+// Inverse of k_row_r2c for rows [0, rows): bins u-major in `in`, output
+// x in [0, W) of each row times `scale` (the crop of updc_core.c:765-766).
+// The imaginary parts of the DC and Nyquist bins are ignored, as FFTW does.
+template <typename T, int NT, int CAP, class Epi>
+__global__ void __launch_bounds__(NT, 1) k_row_c2r(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ post, const cx<T> *__restrict__ in,
+                                                int ldi, size_t in_batch_stride, int rows, int W, int B, T scale, Epi epi) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
+    const int M = plan->n;
+    const int y0 = blockIdx.x * B;
+    const int nb = min(B, rows - y0);
+    const int kexp = blockIdx.y;
+    in += kexp * in_batch_stride;
+    for (int i = threadIdx.x; i < M * B; i += NT) {
+        const int k = i / B, b = i - k * B;
+        cx<T> Zp = {0, 0};
+        if (b < nb) {
+            const int y = y0 + b;
+            cx<T> X = in[(size_t)k * ldi + y];
+            cx<T> Xm = in[(size_t)(M - k) * ldi + y];
+            if (k == 0) { X.y = 0; Xm.y = 0; }
+            const cx<T> S = {X.x + Xm.x, X.y - Xm.y};
+            const cx<T> D = {X.x - Xm.x, X.y + Xm.y};
+            const cx<T> w = post[k];
+            const cx<T> Q = fmulc_conj(D, w);
+            Zp = {S.x - Q.y, S.y + Q.x};
+        }
+        buf[b * M + k] = Zp;
+    }
+    __syncthreads();
+    fft_batch<true, NT, CAP>(buf, B, plan);
+    for (int i = threadIdx.x; i < nb * W; i += NT) {
+        const int b = i / W, x = i - b * W;
+        const cx<T> z = buf[b * M + (x >> 1)];
+        epi(kexp, y0 + b, x, mul_scale((x & 1) ? z.y : z.x, scale));
+    }
+}
+
+
+// ---------------------------------------------------------------------------- columns
+// Forward model for every exposure from the estimate's row-pass intermediate:
+//   Xhat[u] = FFT_y(Rx[u]);  Y_k[u] = IFFT_y(Xhat[u] * K_k[u]) for y < rows_out.
+// The product is (ac - bd, ad + bc) (updc_core.c:753-759).  Xhat never leaves
+// the block: it is kept in shared memory (or in `aux` when it does not fit).
+// All transforms go through one forward-FFT call site; the inverse is
+// conj(FFT(conj(.))), which keeps a single inlined copy of the FFT (two
+// copies make ptxas spill).
+template <typename T, int NT, int CAP>
+__global__ void __launch_bounds__(NT, 1) k_col_forward(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ rx, int ldr, int rows_in,
+                                                    const cx<T> *__restrict__ khat, size_t khat_stride, int nexp,
+                                                    cx<T> *__restrict__ y, int ldy, size_t y_stride, int rows_out,
+                                                    int nu, cx<T> *aux) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
+    const int n = plan->n;
+    const int u = blockIdx.x;
+    cx<T> *xh = aux ? aux + (size_t)u * n : buf + ((n * sizeof(cx<T>) + 15) / 16) * (16 / sizeof(cx<T>));
+    const cx<T> *src = rx + (size_t)u * ldr;
+#pragma unroll 1
+    for (int it = 0; it <= nexp; ++it) {
+        if (it == 0) {
+            for (int v = threadIdx.x; v < n; v += NT) buf[v] = v < rows_in ? src[v] : cx<T>{0, 0};
+        } else {
+            const cx<T> *kr = khat + (it - 1) * khat_stride + (size_t)u * n;
+            for (int v = threadIdx.x; v < n; v += NT) {
+                const cx<T> p = cmul(xh[v], kr[v]);
+                buf[v] = {p.x, -p.y};
+            }
+        }
+        __syncthreads();
+        fft_batch<false, NT, CAP>(buf, 1, plan);
+        if (it == 0) {
+            for (int v = threadIdx.x; v < n; v += NT) xh[v] = buf[v];
+        } else {
+            cx<T> *dst = y + (it - 1) * y_stride + (size_t)u * ldy;
+            for (int v = threadIdx.x; v < rows_out; v += NT) dst[v] = {buf[v].x, -buf[v].y};
+        }
+        __syncthreads();
+    }
+    (void)nu;
+}
+
+// Cross-exposure accumulation policies for the adjoint sum
+//   acc += (a c + b d, b c - a d)   (updc_core.c:988-995)
+template <typename T> struct AccPlain {  // reference order, working precision
+    using S = cx<T>;
+    __device__ __forceinline__ static void zero(S &s) { s = {0, 0}; }
+    __device__ __forceinline__ static void add(S &s, cx<float> a, cx<float> c) {
+        s.x = __fadd_rn(s.x, __fadd_rn(__fmul_rn(a.x, c.x), __fmul_rn(a.y, c.y)));
+        s.y = __fadd_rn(s.y, __fsub_rn(__fmul_rn(a.y, c.x), __fmul_rn(a.x, c.y)));
+    }
+    __device__ __forceinline__ static void add(S &s, cx<double> a, cx<double> c) {
+        s.x = __dadd_rn(s.x, __dadd_rn(__dmul_rn(a.x, c.x), __dmul_rn(a.y, c.y)));
+        s.y = __dadd_rn(s.y, __dsub_rn(__dmul_rn(a.y, c.x), __dmul_rn(a.x, c.y)));
+    }
+    __device__ __forceinline__ static cx<T> get(const S &s) { return s; }
+};
+struct AccF64 {  // FP32 operands, FP64 products and sum
+    using S = cx<double>;
+    __device__ __forceinline__ static void zero(S &s) { s = {0, 0}; }
+    __device__ __forceinline__ static void add(S &s, cx<float> a, cx<float> c) {
+        const double ax = a.x, ay = a.y, cxr = c.x, cy = c.y;
+        s.x += ax * cxr + ay * cy;
+        s.y += ay * cxr - ax * cy;
+    }
+    __device__ __forceinline__ static cx<float> get(const S &s) { return {(float)s.x, (float)s.y}; }
+};
+struct AccKahan {  // FP32 products, Kahan-compensated FP32 sum
+    struct S { float sx, cx_, sy, cy; };
+    __device__ __forceinline__ static void zero(S &s) { s = {0, 0, 0, 0}; }
+    __device__ __forceinline__ static void kadd(float &sum, float &c, float v) {
+        const float y = __fsub_rn(v, c);
+        const float t = __fadd_rn(sum, y);
+        c = __fsub_rn(__fsub_rn(t, sum), y);
+        sum = t;
+    }
+    __device__ __forceinline__ static void add(S &s, cx<float> a, cx<float> c) {
+        kadd(s.sx, s.cx_, __fadd_rn(__fmul_rn(a.x, c.x), __fmul_rn(a.y, c.y)));
+        kadd(s.sy, s.cy, __fsub_rn(__fmul_rn(a.y, c.x), __fmul_rn(a.x, c.y)));
+    }
+    __device__ __forceinline__ static cx<float> get(const S &s) { return {s.sx, s.sy}; }
+};
+
+// Adjoint for every exposure:  C[u] = IFFT_y( sum_k conj(K_k[u]) * FFT_y(Rs_k[u]) )
+// for y < rows_out.  The sum over k runs in exposure order inside the block;
+// the final inverse goes through the same forward-FFT call site as
+// conj(FFT(conj(.))).
+template <typename T, class Acc, int NT, int CAP>
+__global__ void __launch_bounds__(NT, 1) k_col_adjoint(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ rs, int ldr, size_t rs_stride,
+                                                    int rows_in, const cx<T> *__restrict__ khat, size_t khat_stride, int nexp,
+                                                    cx<T> *__restrict__ c, int ldc, int rows_out, typename Acc::S *aux) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
+    const int n = plan->n;
+    const int u = blockIdx.x;
+    typename Acc::S *acc = aux ? aux + (size_t)u * n
+                               : reinterpret_cast<typename Acc::S *>(smem_raw + ((n * sizeof(cx<T>) + 15) / 16) * 16);
+    for (int v = threadIdx.x; v < n; v += NT) Acc::zero(acc[v]);
+#pragma unroll 1
+    for (int it = 0; it <= nexp; ++it) {
+        if (it < nexp) {
+            const cx<T> *src = rs + it * rs_stride + (size_t)u * ldr;
+            for (int v = threadIdx.x; v < n; v += NT) buf[v] = v < rows_in ? src[v] : cx<T>{0, 0};
+        } else {
+            for (int v = threadIdx.x; v < n; v += NT) {
+                const cx<T> a = Acc::get(acc[v]);
+                buf[v] = {a.x, -a.y};
+            }
+        }
+        __syncthreads();
+        fft_batch<false, NT, CAP>(buf, 1, plan);
+        if (it < nexp) {
+            const cx<T> *kr = khat + it * khat_stride + (size_t)u * n;
+            for (int v = threadIdx.x; v < n; v += NT) Acc::add(acc[v], buf[v], kr[v]);
+        } else {
+            cx<T> *dst = c + (size_t)u * ldc;
+            for (int v = threadIdx.x; v < rows_out; v += NT) dst[v] = {buf[v].x, -buf[v].y};
+        }
+        __syncthreads();
+    }
+}
+
+// Plain column transform (setup: PSF spectra and generic 2-D transforms).
+template <typename T, int NT, int CAP, bool INV>
+__global__ void __launch_bounds__(NT, 1) k_col_fft(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ in, int ldi, int rows_in,
+                                                cx<T> *__restrict__ out, int ldo, int rows_out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
+    const int n = plan->n;
+    const int u = blockIdx.x;
+    const cx<T> *src = in + (size_t)u * ldi;
+    for (int v = threadIdx.x; v < n; v += NT) buf[v] = v < rows_in ? src[v] : cx<T>{0, 0};
+    __syncthreads();
+    fft_batch<INV, NT, CAP>(buf, 1, plan);
+    cx<T> *dst = out + (size_t)u * ldo;
+    for (int v = threadIdx.x; v < rows_out; v += NT) dst[v] = buf[v];
+}
+
+}  // namespace updc

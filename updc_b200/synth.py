@@ -74,8 +74,15 @@ WORKLOADS: Dict[str, Workload] = {
     "small": Workload("small", 96, 80, 44, 36, 3, 15, "gauss_moffat", 12, 3, 4, seed=3),
     "medium": Workload("medium", 512, 512, 256, 256, 4, 65, "gauss_moffat", 200, 40, 6,
                        dither_max=4.0, distortion=True, seed=1),
-    "abs32": Workload("abs32", 66000, 6, 6, 2, 2, 3, "gauss_moffat", 3, 0, 2,
-                      scale=2.0, dither_max=0.5, seed=5),
+    # detector pixels 20 target pixels tall: a stencil spans ~20 rows of a
+    # 3400-wide grid (> 65535 indices), forcing ABS32 on a grid the engine's
+    # single-block row transform holds
+    "abs32": Workload("abs32", 3400, 48, 6, 2, 2, 3, "gauss_moffat", 3, 0, 2,
+                      scale=20.0, dither_max=0.5, seed=5),
+    # the reference's own ABS32 validation geometry (target width 70000 class);
+    # CPU oracle only: its rows exceed the GPU row-transform capacity
+    "abs32_wide": Workload("abs32_wide", 66000, 6, 6, 2, 2, 3, "gauss_moffat", 3, 0, 2,
+                           scale=2.0, dither_max=0.5, seed=5),
 }
 
 
