@@ -66,10 +66,19 @@ def test_oracle_reproduces_golden(oracle, case, tmp_path):
 @pytest.mark.gpu
 @pytest.mark.parametrize("case", CASES)
 @pytest.mark.parametrize("form", ["fp32", "fp32-reference"])
-def test_engine_matches_golden(engine_lib, case, form, tmp_path):
+def test_engine_matches_golden(engine_lib, oracle, case, form, tmp_path):
+    """x within 1e-5 relative RMS of the reference after every iteration.  The
+    forced-FreezeMu case is ill-conditioned (ratios y/raw_mu with raw_mu close
+    to 0 after cancellation against the -100 background): there even the exact
+    FP64 oracle drifts from the FP32 reference by ~5e-5 after one iteration and
+    ~1e-2 after four.  For it both FP32 solvers are compared with the FP64
+    oracle: the engine's error must stay within 20x the reference core's own
+    FP32 error (floor 1e-5)."""
     from updc_b200.engine import Engine
     meta, manifest, rows = _stage(case, tmp_path)
     W, H, iw, ih, n, its = (meta[k] for k in ("W", "H", "iw", "ih", "nexp", "iterations"))
+    fw, fh = meta["fft_shape_reference"]
+    s64 = oracle.Solver(str(manifest), W, H, iw, ih, n, fw, fh, precision=64)
     golden_links = []
     for row in rows:
         p = Path(row.links)
@@ -85,7 +94,13 @@ def test_engine_matches_golden(engine_lib, case, form, tmp_path):
     mine = []
     for it in range(1, its + 1):
         st = e.iterate(1)[0]
+        s64.iterate(1)
         ref = np.fromfile(tmp_path / f"ref_{it:02d}.bin", np.float32).reshape(H, W)
-        assert rel_rms(e.plane("estimate"), ref) <= 1e-5
+        if meta["background_override"] is None:
+            assert rel_rms(e.plane("estimate"), ref) <= 1e-5, it
+        else:
+            ref_err = rel_rms(ref, s64.estimate)
+            ours = rel_rms(e.plane("estimate"), s64.estimate)
+            assert ours <= max(1e-5, 20.0 * ref_err), (it, ours, ref_err)
         mine += [(int(st.new_frozen[k]), int(st.total_frozen[k])) for k in range(n)]
     assert mine == [(a, b) for a, b, _ in _golden_rows(tmp_path)]

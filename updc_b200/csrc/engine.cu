@@ -66,6 +66,8 @@ template <typename T> std::vector<cx<T>> fft_make_table(int n, FftPlan &plan) {
         plan.radix[s] = R;
         plan.ns[s] = ns;
         plan.twoff[s] = (int)tab.size();
+        plan.ns_div[s] = FastDiv((uint32_t)ns);
+        plan.nb_div[s] = FastDiv((uint32_t)(n / R));
         for (int k = 0; k < ns; ++k)
             for (int r = 1; r < R; ++r) {
                 const double a = -two_pi * (double)r * (double)k / ((double)ns * (double)R);
@@ -81,12 +83,20 @@ template std::vector<cx<double>> fft_make_table<double>(int, FftPlan &);
 
 namespace {
 
+// Threads per block of the spectral kernels: 512 (two blocks per SM) except
+// the FP32 adjoint column kernel, whose accumulator plane limits it to one
+// block per SM and which therefore runs 1024 threads (FP64 butterflies need
+// the 128-register budget of 512-thread blocks).
 constexpr int NT = 512;
+template <typename T> struct NtAdj {
+    static constexpr int value = sizeof(T) == 4 ? 1024 : 512;
+};
 constexpr size_t SMEM_LIMIT = 227 * 1024;
 
+// Shared-memory capacity (complex elements) of the FFT instantiations.
 template <typename T> struct Caps;
 template <> struct Caps<float> {
-    static constexpr int ROW = 11264;
+    static constexpr int ROW = 5632;
     static constexpr int COL_S = 5632;
     static constexpr int COL_L = 11264;
 };
@@ -533,8 +543,8 @@ template <typename T> class EngineImpl final : public Engine {
         if constexpr (sizeof(typename Acc::S) > 0) {
             if constexpr (std::is_same<Acc, AccPlain<T>>::value || sizeof(T) == 4) {
                 const size_t s = adj_smem<Acc>();
-                set_smem(k_col_adjoint<T, Acc, NT, Caps<T>::COL_S>, s);
-                set_smem(k_col_adjoint<T, Acc, NT, Caps<T>::COL_L>, s);
+                set_smem(k_col_adjoint<T, Acc, NtAdj<T>::value,Caps<T>::COL_S>, s);
+                set_smem(k_col_adjoint<T, Acc, NtAdj<T>::value,Caps<T>::COL_L>, s);
             }
         }
     }
@@ -574,9 +584,9 @@ template <typename T> class EngineImpl final : public Engine {
         }
         const size_t s = adj_smem<Acc>();
         if (FH_ <= Caps<T>::COL_S)
-            k_col_adjoint<T, Acc, NT, Caps<T>::COL_S><<<(unsigned)nu, NT, s, stream_>>>(d_plan_h_, rs_, H_, nu * H_, H_, khat, nu * FH_, nexp_, cr_, H_, H_, aux);
+            k_col_adjoint<T, Acc, NtAdj<T>::value,Caps<T>::COL_S><<<(unsigned)nu, NtAdj<T>::value, s, stream_>>>(d_plan_h_, rs_, H_, nu * H_, H_, khat, nu * FH_, nexp_, cr_, H_, H_, aux);
         else
-            k_col_adjoint<T, Acc, NT, Caps<T>::COL_L><<<(unsigned)nu, NT, s, stream_>>>(d_plan_h_, rs_, H_, nu * H_, H_, khat, nu * FH_, nexp_, cr_, H_, H_, aux);
+            k_col_adjoint<T, Acc, NtAdj<T>::value,Caps<T>::COL_L><<<(unsigned)nu, NtAdj<T>::value, s, stream_>>>(d_plan_h_, rs_, H_, nu * H_, H_, khat, nu * FH_, nexp_, cr_, H_, H_, aux);
         UPDC_CUDA(cudaGetLastError());
     }
     void launch_col_adjoint() {
@@ -931,11 +941,11 @@ template <typename T> class EngineImpl final : public Engine {
         cx<D> *aux = aux_needed ? dalloc<cx<D>>(nu * FH_, nullptr) : nullptr;
         const size_t s = aux_needed ? b : 2 * b;
         if (FH_ <= Caps<D>::COL_S) {
-            set_smem(k_col_adjoint<D, AccPlain<D>, NT, Caps<D>::COL_S>, s);
-            k_col_adjoint<D, AccPlain<D>, NT, Caps<D>::COL_S><<<(unsigned)nu, NT, s, stream_>>>(dph, rs, H_, nu * H_, H_, kd, nu * FH_, nexp_, cr, H_, H_, aux);
+            set_smem(k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_S>, s);
+            k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_S><<<(unsigned)nu, NtAdj<D>::value, s, stream_>>>(dph, rs, H_, nu * H_, H_, kd, nu * FH_, nexp_, cr, H_, H_, aux);
         } else {
-            set_smem(k_col_adjoint<D, AccPlain<D>, NT, Caps<D>::COL_L>, s);
-            k_col_adjoint<D, AccPlain<D>, NT, Caps<D>::COL_L><<<(unsigned)nu, NT, s, stream_>>>(dph, rs, H_, nu * H_, H_, kd, nu * FH_, nexp_, cr, H_, H_, aux);
+            set_smem(k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_L>, s);
+            k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_L><<<(unsigned)nu, NtAdj<D>::value, s, stream_>>>(dph, rs, H_, nu * H_, H_, kd, nu * FH_, nexp_, cr, H_, H_, aux);
         }
         D *den = dalloc<D>(nout_, nullptr);
         set_smem(k_row_c2r<D, NT, Caps<D>::ROW, PlaneStore<D>>, rsm);

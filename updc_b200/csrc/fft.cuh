@@ -18,12 +18,34 @@ namespace updc {
 
 constexpr int FFT_MAX_STAGES = 24;
 
+// Division by a run-time constant d for x < 2^31: q = (umulhi(x, mul) + x) >> shift
+// with shift = ceil(log2 d) and mul = floor(2^32 (2^shift - d) / d) + 1
+// (the round-up method for unsigned division by invariant integers).
+struct FastDiv {
+    uint32_t d = 1, mul = 1, shift = 0;
+    FastDiv() = default;
+    explicit FastDiv(uint32_t div) : d(div) {
+        shift = 0;
+        while ((1ull << shift) < div) ++shift;
+        mul = (uint32_t)((((1ull << 32) * ((1ull << shift) - div)) / div) + 1);
+    }
+    __host__ __device__ __forceinline__ uint32_t div(uint32_t x) const {
+#ifdef __CUDA_ARCH__
+        return (__umulhi(x, mul) + x) >> shift;
+#else
+        return (uint32_t)((((uint64_t)x * mul >> 32) + x) >> shift);
+#endif
+    }
+};
+
 struct FftPlan {
     int n = 0;
     int nstage = 0;
     int radix[FFT_MAX_STAGES] = {};
     int ns[FFT_MAX_STAGES] = {};
     int twoff[FFT_MAX_STAGES] = {};
+    FastDiv ns_div[FFT_MAX_STAGES];   // division by Ns
+    FastDiv nb_div[FFT_MAX_STAGES];   // division by n / radix
     const void *tw = nullptr;  // device table of cx<T>, forward sign
 };
 
@@ -157,20 +179,29 @@ template <bool INV, typename T> struct Dft<7, INV, T> {
 
 // ----------------------------------------------------------------------------- stages
 template <int R, int K, bool INV, int NT, typename T>
-__device__ __forceinline__ void fft_stage(cx<T> *buf, int n, int batch, int Ns, const cx<T> *__restrict__ tw) {
+__device__ __forceinline__ void fft_stage(cx<T> *buf, int n, int batch, int Ns, FastDiv ns_div, FastDiv nb_div,
+                                          const cx<T> *__restrict__ tw) {
     const int nb = n / R;
     const int total = nb * batch;
     const int tid = threadIdx.x;
+    // v is defined on every path: a conditionally defined array becomes live
+    // around the back-edge of any loop that calls the FFT, which keeps every
+    // stage's registers live at once and spills.
     cx<T> v[K][R];
     int ob[K];
+#pragma unroll
+    for (int kk = 0; kk < K; ++kk) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[kk][r] = cx<T>{T(0), T(0)};
+    }
 #pragma unroll
     for (int kk = 0; kk < K; ++kk) {
         const int b = tid + kk * NT;
         ob[kk] = -1;
         if (b < total) {
-            const int row = b / nb;
+            const int row = batch == 1 ? 0 : (int)nb_div.div((uint32_t)b);
             const int j = b - row * nb;
-            const int k = j % Ns;
+            const int k = j - (int)ns_div.div((uint32_t)j) * Ns;
             const cx<T> *base = buf + row * n;
 #pragma unroll
             for (int r = 0; r < R; ++r) v[kk][r] = base[j + r * nb];
@@ -202,24 +233,44 @@ template <int R, int NT, int CAP> struct StageK {
     static constexpr int value = (CAP / R + NT - 1) / NT;
 };
 
+__device__ __forceinline__ FastDiv FastDiv_v(const volatile FastDiv &v) {
+    FastDiv r;
+    r.d = v.d;
+    r.mul = v.mul;
+    r.shift = v.shift;
+    return r;
+}
+
+// Copies a plan from device memory into the block's shared copy.  Kernels
+// keep the plan in shared memory: indexing a kernel-parameter array
+// dynamically would force a local copy of the structure, and reading the
+// fields from global memory on every stage exposes a full memory latency.
+__device__ __forceinline__ void load_plan(const FftPlan *__restrict__ g, FftPlan *s) {
+    const int *src = reinterpret_cast<const int *>(g);
+    int *dst = reinterpret_cast<int *>(s);
+    for (int i = threadIdx.x; i < (int)(sizeof(FftPlan) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+}
+
 // Transforms `batch` sequences of length plan.n stored back to back in buf
-// (batch * n <= CAP).  Every thread of the block must call this.
-// The plan lives in device global memory: its fields are read with uniform
-// loads (indexing a kernel-parameter array dynamically would force a local
-// copy of the whole structure).  Stages are ordered by radix (fft_factor), and
+// (batch * n <= CAP).  Every thread of the block must call this; `plan` points
+// to the block's shared copy.  Stages are ordered by radix (fft_factor), and
 // each radix gets its own loop so that only one radix's registers are live at
 // a time (a single switch inside one loop makes ptxas spill).
 template <bool INV, int NT, int CAP, typename T>
-__device__ __forceinline__ void fft_batch(cx<T> *buf, int batch, const FftPlan *__restrict__ plan) {
-    // volatile reads keep the per-stage fields from being hoisted out of the
-    // callers' loops (a hoisted copy of the whole plan would spill)
+__device__ __forceinline__ void fft_batch(cx<T> *buf, int batch, const FftPlan *plan) {
+    // volatile (shared-memory) reads keep the per-stage fields from being
+    // hoisted out of the callers' loops (a hoisted copy of the whole plan
+    // would spill)
     const volatile FftPlan *vp = plan;
     const cx<T> *tw = reinterpret_cast<const cx<T> *>(vp->tw);
     const int n = vp->n, nstage = vp->nstage;
     int s = 0;
 #define UPDC_FFT_RUN(R)                                                                                   \
     _Pragma("unroll 1") while (s < nstage && vp->radix[s] == R) {                                                           \
-        fft_stage<R, StageK<R, NT, CAP>::value, INV, NT>(buf, n, batch, vp->ns[s], tw + vp->twoff[s]);   \
+        fft_stage<R, StageK<R, NT, CAP>::value, INV, NT>(buf, n, batch, vp->ns[s],                       \
+                                                         FastDiv_v(vp->ns_div[s]), FastDiv_v(vp->nb_div[s]), \
+                                                         tw + vp->twoff[s]);                             \
         ++s;                                                                                             \
     }
     UPDC_FFT_RUN(8)

@@ -10,6 +10,14 @@
 
 namespace updc {
 
+// FP32 blocks of <= 512 threads over at most 5632 complex elements are
+// compiled for two resident blocks per SM (64 registers a thread); FP64,
+// larger transforms and larger blocks for one (their butterflies need up to
+// 128 registers).
+template <int NT, int CAP, typename T> struct MinBlocks {
+    static constexpr int value = (NT <= 512 && CAP <= 5632 && sizeof(T) == 4) ? 2 : 1;
+};
+
 // ---------------------------------------------------------------------------- loaders
 template <typename T> struct PlaneLoader {
     const T *p;
@@ -39,11 +47,13 @@ template <typename T> struct PsfLoader {
 // transformed along x with an M-point complex FFT of z[m] = x[2m] + i x[2m+1]
 // and the split z -> X post-processing; bins are stored u-major.
 template <typename T, int NT, int CAP, class Loader>
-__global__ void __launch_bounds__(NT, 1) k_row_r2c(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ post, Loader ld, int W,
+__global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_row_r2c(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ post, Loader ld, int W,
                                                 int rows, int B, cx<T> *__restrict__ out, int ldo, size_t out_batch_stride) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
-    const int M = plan->n;
+    __shared__ FftPlan s_plan;
+    load_plan(plan, &s_plan);
+    const int M = s_plan.n;
     const int y0 = blockIdx.x * B;
     const int nb = min(B, rows - y0);
     out += blockIdx.y * out_batch_stride;
@@ -58,7 +68,7 @@ __global__ void __launch_bounds__(NT, 1) k_row_r2c(const FftPlan *__restrict__ p
         buf[i] = {a, c};
     }
     __syncthreads();
-    fft_batch<false, NT, CAP>(buf, B, plan);
+    fft_batch<false, NT, CAP>(buf, B, &s_plan);
     const T half = T(0.5);
     for (int i = threadIdx.x; i < (M + 1) * B; i += NT) {
         const int u = i / B, b = i - u * B;
@@ -88,11 +98,13 @@ template <typename T> struct PlaneStore {
 // x in [0, W) of each row times `scale` (the crop of updc_core.c:765-766).
 // The imaginary parts of the DC and Nyquist bins are ignored, as FFTW does.
 template <typename T, int NT, int CAP, class Epi>
-__global__ void __launch_bounds__(NT, 1) k_row_c2r(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ post, const cx<T> *__restrict__ in,
+__global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_row_c2r(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ post, const cx<T> *__restrict__ in,
                                                 int ldi, size_t in_batch_stride, int rows, int W, int B, T scale, Epi epi) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
-    const int M = plan->n;
+    __shared__ FftPlan s_plan;
+    load_plan(plan, &s_plan);
+    const int M = s_plan.n;
     const int y0 = blockIdx.x * B;
     const int nb = min(B, rows - y0);
     const int kexp = blockIdx.y;
@@ -114,7 +126,7 @@ __global__ void __launch_bounds__(NT, 1) k_row_c2r(const FftPlan *__restrict__ p
         buf[b * M + k] = Zp;
     }
     __syncthreads();
-    fft_batch<true, NT, CAP>(buf, B, plan);
+    fft_batch<true, NT, CAP>(buf, B, &s_plan);
     for (int i = threadIdx.x; i < nb * W; i += NT) {
         const int b = i / W, x = i - b * W;
         const cx<T> z = buf[b * M + (x >> 1)];
@@ -132,13 +144,15 @@ __global__ void __launch_bounds__(NT, 1) k_row_c2r(const FftPlan *__restrict__ p
 // conj(FFT(conj(.))), which keeps a single inlined copy of the FFT (two
 // copies make ptxas spill).
 template <typename T, int NT, int CAP>
-__global__ void __launch_bounds__(NT, 1) k_col_forward(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ rx, int ldr, int rows_in,
+__global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_forward(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ rx, int ldr, int rows_in,
                                                     const cx<T> *__restrict__ khat, size_t khat_stride, int nexp,
                                                     cx<T> *__restrict__ y, int ldy, size_t y_stride, int rows_out,
                                                     int nu, cx<T> *aux) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
-    const int n = plan->n;
+    __shared__ FftPlan s_plan;
+    load_plan(plan, &s_plan);
+    const int n = s_plan.n;
     const int u = blockIdx.x;
     cx<T> *xh = aux ? aux + (size_t)u * n : buf + ((n * sizeof(cx<T>) + 15) / 16) * (16 / sizeof(cx<T>));
     const cx<T> *src = rx + (size_t)u * ldr;
@@ -154,7 +168,7 @@ __global__ void __launch_bounds__(NT, 1) k_col_forward(const FftPlan *__restrict
             }
         }
         __syncthreads();
-        fft_batch<false, NT, CAP>(buf, 1, plan);
+        fft_batch<false, NT, CAP>(buf, 1, &s_plan);
         if (it == 0) {
             for (int v = threadIdx.x; v < n; v += NT) xh[v] = buf[v];
         } else {
@@ -212,12 +226,14 @@ struct AccKahan {  // FP32 products, Kahan-compensated FP32 sum
 // the final inverse goes through the same forward-FFT call site as
 // conj(FFT(conj(.))).
 template <typename T, class Acc, int NT, int CAP>
-__global__ void __launch_bounds__(NT, 1) k_col_adjoint(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ rs, int ldr, size_t rs_stride,
+__global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_adjoint(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ rs, int ldr, size_t rs_stride,
                                                     int rows_in, const cx<T> *__restrict__ khat, size_t khat_stride, int nexp,
                                                     cx<T> *__restrict__ c, int ldc, int rows_out, typename Acc::S *aux) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
-    const int n = plan->n;
+    __shared__ FftPlan s_plan;
+    load_plan(plan, &s_plan);
+    const int n = s_plan.n;
     const int u = blockIdx.x;
     typename Acc::S *acc = aux ? aux + (size_t)u * n
                                : reinterpret_cast<typename Acc::S *>(smem_raw + ((n * sizeof(cx<T>) + 15) / 16) * 16);
@@ -234,7 +250,7 @@ __global__ void __launch_bounds__(NT, 1) k_col_adjoint(const FftPlan *__restrict
             }
         }
         __syncthreads();
-        fft_batch<false, NT, CAP>(buf, 1, plan);
+        fft_batch<false, NT, CAP>(buf, 1, &s_plan);
         if (it < nexp) {
             const cx<T> *kr = khat + it * khat_stride + (size_t)u * n;
             for (int v = threadIdx.x; v < n; v += NT) Acc::add(acc[v], buf[v], kr[v]);
@@ -248,16 +264,18 @@ __global__ void __launch_bounds__(NT, 1) k_col_adjoint(const FftPlan *__restrict
 
 // Plain column transform (setup: PSF spectra and generic 2-D transforms).
 template <typename T, int NT, int CAP, bool INV>
-__global__ void __launch_bounds__(NT, 1) k_col_fft(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ in, int ldi, int rows_in,
+__global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_fft(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ in, int ldi, int rows_in,
                                                 cx<T> *__restrict__ out, int ldo, int rows_out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
-    const int n = plan->n;
+    __shared__ FftPlan s_plan;
+    load_plan(plan, &s_plan);
+    const int n = s_plan.n;
     const int u = blockIdx.x;
     const cx<T> *src = in + (size_t)u * ldi;
     for (int v = threadIdx.x; v < n; v += NT) buf[v] = v < rows_in ? src[v] : cx<T>{0, 0};
     __syncthreads();
-    fft_batch<INV, NT, CAP>(buf, 1, plan);
+    fft_batch<INV, NT, CAP>(buf, 1, &s_plan);
     cx<T> *dst = out + (size_t)u * ldo;
     for (int v = threadIdx.x; v < rows_out; v += NT) dst[v] = buf[v];
 }

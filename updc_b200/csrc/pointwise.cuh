@@ -54,6 +54,39 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
 }
 
 // ---------------------------------------------------------------------------- detector
+// Warp-cooperative link staging.  A warp owns 32 consecutive detector pixels;
+// their links occupy one contiguous range of the LinkMap, which the warp
+// copies into shared memory with coalesced loads (one lane per link) before
+// each lane walks its own pixel's links from there.  Ranges longer than
+// DET_LCAP links fall back to direct loads for that tile.
+constexpr int DET_WARPS = 8;
+constexpr int DET_LCAP = 384;
+
+template <typename T> struct LinkSum {
+    T s = T(0), c = T(0);
+    template <bool COMP> __device__ __forceinline__ void add(float f, T bl) {
+        if (!COMP) {
+            s = fma_rn((T)f, bl, s);
+        } else {  // Dot2: error-free product and sum
+            const T a = (T)f;
+            const T h = mul_rn(a, bl);
+            const T r = fma_rn(a, bl, -h);
+            const T s2 = add_rn(s, h);
+            const T bb = sub_rn(s2, s);
+            const T q = add_rn(sub_rn(s, sub_rn(s2, bb)), sub_rn(h, bb));
+            s = s2;
+            c = add_rn(c, add_rn(q, r));
+        }
+    }
+    template <bool COMP> __device__ __forceinline__ T finish(T offset) const {
+        if (!COMP) return add_rn(s, offset);
+        const T s2 = add_rn(s, offset);
+        const T bb = sub_rn(s2, s);
+        const T q = add_rn(sub_rn(s, sub_rn(s2, bb)), sub_rn(offset, bb));
+        return add_rn(s2, add_rn(c, q));
+    }
+};
+
 // The fused detector loop of updc_core.c:1152-1176 for exposure blockIdx.y:
 //   pred = sum_z fmaf(frac[z], blur[t(z)], pred) in link order;
 //   raw_mu = pred + (background + pedestal);  FreezeMu;  ratio;  wr = W * ratio.
@@ -62,78 +95,83 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
 // Dot2) and raw_mu its correctly rounded sum with the offset, so the
 // FreezeMu threshold is decided on a compensated raw_mu.
 template <typename T, bool COMP>
-__global__ void __launch_bounds__(256) k_detector(const ExpDesc<T> *__restrict__ exps, size_t nin, size_t nout,
-                                                  const T *__restrict__ blur_all, T *__restrict__ wr_all,
-                                                  ExpStats *__restrict__ stats, unsigned long long *__restrict__ err) {
+__global__ void __launch_bounds__(DET_WARPS * 32) k_detector(const ExpDesc<T> *__restrict__ exps, size_t nin, size_t nout,
+                                                           const T *__restrict__ blur_all, T *__restrict__ wr_all,
+                                                           ExpStats *__restrict__ stats, unsigned long long *__restrict__ err) {
+    __shared__ uint32_t s_idx[DET_WARPS][DET_LCAP];
+    __shared__ float s_frac[DET_WARPS][DET_LCAP];
     const int k = blockIdx.y;
     const ExpDesc<T> e = exps[k];
     const T *blur = blur_all + k * nout;
     T *wr = wr_all + k * nin;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned long long nnew = 0, ntot = 0, mn = ~0ull;
-    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < nin; p += (size_t)gridDim.x * blockDim.x) {
-        const T w = e.wht[p];
-        const uint32_t z0 = e.off[p], z1 = e.off[p + 1];
-        T out = T(0);
-        if (w > T(0) && z0 != z1) {
-            T raw_mu;
-            if (!COMP) {
-                T pred = T(0);
-                if (e.delta16) {
-                    const uint32_t b = e.base[p];
-                    for (uint32_t z = z0; z < z1; ++z) pred = fma_rn((T)e.frac[z], blur[b + (uint32_t)e.delta[z]], pred);
-                } else {
-                    for (uint32_t z = z0; z < z1; ++z) pred = fma_rn((T)e.frac[z], blur[e.tgt[z]], pred);
-                }
-                raw_mu = add_rn(pred, e.mean_offset);
-            } else {
-                T s = T(0), c = T(0);
-                for (uint32_t z = z0; z < z1; ++z) {
-                    const uint32_t t = e.delta16 ? e.base[p] + (uint32_t)e.delta[z] : e.tgt[z];
-                    const T a = (T)e.frac[z], bl = blur[t];
-                    const T h = mul_rn(a, bl);
-                    const T r = fma_rn(a, bl, -h);
-                    const T s2 = add_rn(s, h);
-                    const T bb = sub_rn(s2, s);
-                    const T q = add_rn(sub_rn(s, sub_rn(s2, bb)), sub_rn(h, bb));
-                    s = s2;
-                    c = add_rn(c, add_rn(q, r));
-                }
-                const T s2 = add_rn(s, e.mean_offset);
-                const T bb = sub_rn(s2, s);
-                const T q = add_rn(sub_rn(s, sub_rn(s2, bb)), sub_rn(e.mean_offset, bb));
-                raw_mu = add_rn(s2, add_rn(c, q));
-            }
-            if (!isfinite(raw_mu)) {
-                record_error(err, STAGE_DETECTOR, (uint64_t)k * nin + p, ERR_NONFINITE_MEAN);
-            } else {
-                const unsigned long long o = double_to_ordered((double)raw_mu);
-                mn = o < mn ? o : mn;
-                uint8_t fz = e.frozen[p];
-                if (!fz && !(raw_mu > T(0))) {
-                    fz = 1;
-                    e.frozen[p] = 1;
-                    ++nnew;
-                }
-                T ratio;
-                if (fz) {
-                    ++ntot;
-                    ratio = T(1);
-                } else {
-                    const T y = add_rn(e.sci[p], e.pedestal);
-                    ratio = div_rn(y, raw_mu);
-                    if (!isfinite(ratio)) record_error(err, STAGE_DETECTOR, (uint64_t)k * nin + p, ERR_NONFINITE_RATIO);
-                }
-                out = mul_rn(w, ratio);
+    const size_t step = (size_t)gridDim.x * DET_WARPS * 32;
+    for (size_t p0 = ((size_t)blockIdx.x * DET_WARPS + warp) * 32; p0 < nin; p0 += step) {
+        const size_t p = p0 + lane;
+        const bool valid = p < nin;
+        const uint32_t z0 = valid ? e.off[p] : 0u, z1 = valid ? e.off[p + 1] : 0u;
+        const int last = (int)min((size_t)31, nin - 1 - p0);
+        const uint32_t zb = __shfl_sync(0xffffffffu, z0, 0);
+        const uint32_t ze = __shfl_sync(0xffffffffu, z1, last);
+        const bool staged = ze - zb <= (uint32_t)DET_LCAP;
+        if (staged) {
+            for (uint32_t i = lane; i < ze - zb; i += 32) {
+                s_frac[warp][i] = e.frac[zb + i];
+                s_idx[warp][i] = e.delta16 ? (uint32_t)e.delta[zb + i] : e.tgt[zb + i];
             }
         }
-        wr[p] = out;
+        __syncwarp();
+        T out = T(0);
+        if (valid) {
+            const T w = e.wht[p];
+            if (w > T(0) && z0 != z1) {
+                const uint32_t bse = e.delta16 ? e.base[p] : 0u;
+                LinkSum<T> acc;
+                if (staged) {
+                    for (uint32_t z = z0; z < z1; ++z) {
+                        const uint32_t j = z - zb;
+                        acc.template add<COMP>(s_frac[warp][j], blur[bse + s_idx[warp][j]]);
+                    }
+                } else {
+                    for (uint32_t z = z0; z < z1; ++z) {
+                        const uint32_t t = e.delta16 ? bse + (uint32_t)e.delta[z] : e.tgt[z];
+                        acc.template add<COMP>(e.frac[z], blur[t]);
+                    }
+                }
+                const T raw_mu = acc.template finish<COMP>(e.mean_offset);
+                if (!isfinite(raw_mu)) {
+                    record_error(err, STAGE_DETECTOR, (uint64_t)k * nin + p, ERR_NONFINITE_MEAN);
+                } else {
+                    const unsigned long long o = double_to_ordered((double)raw_mu);
+                    mn = o < mn ? o : mn;
+                    uint8_t fz = e.frozen[p];
+                    if (!fz && !(raw_mu > T(0))) {
+                        fz = 1;
+                        e.frozen[p] = 1;
+                        ++nnew;
+                    }
+                    T ratio;
+                    if (fz) {
+                        ++ntot;
+                        ratio = T(1);
+                    } else {
+                        const T y = add_rn(e.sci[p], e.pedestal);
+                        ratio = div_rn(y, raw_mu);
+                        if (!isfinite(ratio)) record_error(err, STAGE_DETECTOR, (uint64_t)k * nin + p, ERR_NONFINITE_RATIO);
+                    }
+                    out = mul_rn(w, ratio);
+                }
+            }
+            wr[p] = out;
+        }
+        __syncwarp();  // the next tile reuses this warp's staging area
     }
     // block reduction of the counters
-    __shared__ unsigned long long s_new[8], s_tot[8], s_min[8];
+    __shared__ unsigned long long s_new[DET_WARPS], s_tot[DET_WARPS], s_min[DET_WARPS];
     nnew = block_sum_warp(nnew);
     ntot = block_sum_warp(ntot);
     mn = warp_min_u64(mn);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (lane == 0) {
         s_new[warp] = nnew;
         s_tot[warp] = ntot;
@@ -142,7 +180,7 @@ __global__ void __launch_bounds__(256) k_detector(const ExpDesc<T> *__restrict__
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned long long a = 0, b = 0, m = ~0ull;
-        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+        for (int i = 0; i < DET_WARPS; ++i) {
             a += s_new[i];
             b += s_tot[i];
             m = s_min[i] < m ? s_min[i] : m;
@@ -156,30 +194,56 @@ __global__ void __launch_bounds__(256) k_detector(const ExpDesc<T> *__restrict__
 // ---------------------------------------------------------------------------- adjoint gather
 // scatter_k[t] = sum over the transposed entries of t, in increasing source
 // pixel order, of fmaf(frac, value[p], acc): the exact sequence of
-// updc_core.c:1173-1176 for target t.  ACC may be wider than T.
+// updc_core.c:1173-1176 for target t.  ACC may be wider than T.  Entries of a
+// warp's 32 consecutive targets are one contiguous range, staged in shared
+// memory with coalesced loads as in k_detector.
+constexpr int GATHER_LCAP = 256;
+
 template <typename T, typename ACC, typename V>
-__global__ void __launch_bounds__(256) k_scatter_t(const ExpDesc<T> *__restrict__ exps, size_t nin, size_t nout,
-                                                   const V *__restrict__ val_all, int use_weight, ACC *__restrict__ out_all) {
+__global__ void __launch_bounds__(DET_WARPS * 32) k_scatter_t(const ExpDesc<T> *__restrict__ exps, size_t nin, size_t nout,
+                                                            const V *__restrict__ val_all, int use_weight,
+                                                            ACC *__restrict__ out_all) {
+    __shared__ uint32_t s_src[DET_WARPS][GATHER_LCAP];
+    __shared__ float s_frac[DET_WARPS][GATHER_LCAP];
     const int k = blockIdx.y;
     const ExpDesc<T> e = exps[k];
     const V *val = use_weight ? nullptr : val_all + k * nin;
     ACC *out = out_all + k * nout;
-    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nout; t += (size_t)gridDim.x * blockDim.x) {
-        const uint32_t a = e.toff[t], b = e.toff[t + 1];
-        ACC acc = ACC(0);
-        for (uint32_t i = a; i < b; ++i) {
-            const uint32_t p = e.tsrc[i];
-            ACC v;
-            if (use_weight) {
-                const T w = e.wht[p];
-                if (!(w > T(0))) continue;
-                v = (ACC)w;
-            } else {
-                v = (ACC)val[p];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const size_t step = (size_t)gridDim.x * DET_WARPS * 32;
+    for (size_t t0 = ((size_t)blockIdx.x * DET_WARPS + warp) * 32; t0 < nout; t0 += step) {
+        const size_t t = t0 + lane;
+        const bool valid = t < nout;
+        const uint32_t a = valid ? e.toff[t] : 0u, b = valid ? e.toff[t + 1] : 0u;
+        const int last = (int)min((size_t)31, nout - 1 - t0);
+        const uint32_t eb = __shfl_sync(0xffffffffu, a, 0);
+        const uint32_t ee = __shfl_sync(0xffffffffu, b, last);
+        const bool staged = ee - eb <= (uint32_t)GATHER_LCAP;
+        if (staged) {
+            for (uint32_t i = lane; i < ee - eb; i += 32) {
+                s_src[warp][i] = e.tsrc[eb + i];
+                s_frac[warp][i] = e.tfrac[eb + i];
             }
-            acc = fma_rn((ACC)e.tfrac[i], v, acc);
         }
-        out[t] = acc;
+        __syncwarp();
+        if (valid) {
+            ACC acc = ACC(0);
+            for (uint32_t i = a; i < b; ++i) {
+                const uint32_t src = staged ? s_src[warp][i - eb] : e.tsrc[i];
+                const float fr = staged ? s_frac[warp][i - eb] : e.tfrac[i];
+                ACC v;
+                if (use_weight) {
+                    const T w = e.wht[src];
+                    if (!(w > T(0))) continue;  // masked pixels are skipped (updc_core.c:1061)
+                    v = (ACC)w;
+                } else {
+                    v = (ACC)val[src];
+                }
+                acc = fma_rn((ACC)fr, v, acc);
+            }
+            out[t] = acc;
+        }
+        __syncwarp();
     }
 }
 
