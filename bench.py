@@ -181,6 +181,35 @@ def reference_arm(args, rank, world):
 
 
 # ----------------------------------------------------------------------------- b200 arm
+def cufft_reference(torch, w, fw, fh, reps=5):
+    """Device time of cuFFT (torch.fft) for one padded R2C of a W x H plane and
+    one C2R with crop, on the FFT grid the engine uses."""
+    x = torch.randn((w.H, w.W), device="cuda", dtype=torch.float32)
+    pad = torch.zeros((fh, fw), device="cuda", dtype=torch.float32)
+    spec = torch.fft.rfft2(pad)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    for _ in range(2):
+        pad[:w.H, :w.W] = x
+        spec = torch.fft.rfft2(pad)
+        _ = torch.fft.irfft2(spec, s=(fh, fw))[:w.H, :w.W].contiguous()
+    torch.cuda.synchronize()
+    ev[0].record()
+    for _ in range(reps):
+        pad[:w.H, :w.W] = x
+        spec = torch.fft.rfft2(pad)
+    ev[1].record()
+    for _ in range(reps):
+        _ = torch.fft.irfft2(spec, s=(fh, fw))[:w.H, :w.W].contiguous()
+    ev[2].record()
+    torch.cuda.synchronize()
+    r2c = ev[0].elapsed_time(ev[1]) / reps
+    c2r = ev[1].elapsed_time(ev[2]) / reps
+    del x, pad, spec
+    torch.cuda.empty_cache()
+    return {"r2c_ms": round(r2c, 4), "c2r_crop_ms": round(c2r, 4), "grid": [fw, fh],
+            "note": "torch.fft (cuFFT) on the same padded grid; comparison only"}
+
+
 def cpu_baseline_sample(ds, w):
     """One iteration of the reference core on the same inputs (rank 0, N=1)."""
     from oracle import oracle as O
@@ -247,6 +276,10 @@ def b200_arm(args, rank, world, local_rank):
     dom = max(stage_ms, key=stage_ms.get)
     peak, peak_kind = measured_peaks()
     achieved = sb[dom] / (stage_ms[dom] * 1e-3) / 1e9
+    # cuFFT (through torch) on the same padded grid, for comparison only: one
+    # zero-padded 2-D R2C of the 4096^2 plane and one C2R + crop, as our
+    # estimate/forward passes do them (not used by the solver)
+    cufft = cufft_reference(torch, w, fw, fh)
     # e2e through the C ABI with pinned host buffers: upload x, one iteration, read x back
     xdt = torch.float64 if args.form == "fp64" else torch.float32
     x = torch.empty((w.H, w.W), dtype=xdt, pin_memory=True).numpy()
@@ -281,6 +314,7 @@ def b200_arm(args, rank, world, local_rank):
         "cpu_baseline": cpu,
         "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": x.itemsize * nout,
                 "d2h_bytes_per_step": x.itemsize * nout},
+        "cufft_reference": cufft,
         "gpu_launches": launches_per_iter * args.steps,
         "clocks": clocks.summary(),
     }

@@ -41,6 +41,7 @@ enum DevErrorCode : uint32_t {
     ERR_NONFINITE_INITIAL = 8,       // "non-finite signed initial estimate"
     ERR_INVALID_PSF_PIXEL = 9,       // "invalid PSF pixel"
     ERR_LINKMAP_TARGET = 10,         // LinkMap target outside the grid (defensive bounds check)
+    ERR_DEVICE_TIMEOUT = 11,         // a bounded device-side wait ran out
 };
 enum DevErrorStage : uint64_t { STAGE_DETECTOR = 1, STAGE_UPDATE = 2, STAGE_SETUP = 3 };
 
@@ -54,8 +55,8 @@ const char *error_message(uint32_t code);
 template <typename T> struct cx { T x, y; };
 
 template <typename T> __host__ __device__ __forceinline__ cx<T> cmk(T a, T b) { return cx<T>{a, b}; }
-template <typename T> __device__ __forceinline__ cx<T> operator+(cx<T> a, cx<T> b) { return {a.x + b.x, a.y + b.y}; }
-template <typename T> __device__ __forceinline__ cx<T> operator-(cx<T> a, cx<T> b) { return {a.x - b.x, a.y - b.y}; }
+template <typename T> __host__ __device__ __forceinline__ cx<T> operator+(cx<T> a, cx<T> b) { return {a.x + b.x, a.y + b.y}; }
+template <typename T> __host__ __device__ __forceinline__ cx<T> operator-(cx<T> a, cx<T> b) { return {a.x - b.x, a.y - b.y}; }
 // (a.x b.x - a.y b.y, a.x b.y + a.y b.x), evaluated without contraction so the
 // FP32 products round like the reference's separate multiplies.
 template <typename T> __device__ __forceinline__ cx<T> cmul(cx<T> a, cx<T> b);
@@ -66,13 +67,13 @@ template <> __device__ __forceinline__ cx<double> cmul(cx<double> a, cx<double> 
     return {__dsub_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)), __dadd_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x))};
 }
 // Fast complex multiply for FFT internals (contraction allowed).
-template <typename T> __device__ __forceinline__ cx<T> fmulc(cx<T> a, cx<T> b) {
+template <typename T> __host__ __device__ __forceinline__ cx<T> fmulc(cx<T> a, cx<T> b) {
     return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
 }
-template <typename T> __device__ __forceinline__ cx<T> fmulc_conj(cx<T> a, cx<T> b) {  // a * conj(b)
+template <typename T> __host__ __device__ __forceinline__ cx<T> fmulc_conj(cx<T> a, cx<T> b) {  // a * conj(b)
     return {a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y};
 }
-template <typename T> __device__ __forceinline__ cx<T> cscale(cx<T> a, T s) { return {a.x * s, a.y * s}; }
+template <typename T> __host__ __device__ __forceinline__ cx<T> cscale(cx<T> a, T s) { return {a.x * s, a.y * s}; }
 
 // ----------------------------------------------------------------------------- misc
 __host__ __device__ inline size_t ceil_div(size_t a, size_t b) { return (a + b - 1) / b; }

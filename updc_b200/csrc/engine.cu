@@ -14,6 +14,32 @@
 
 namespace updc {
 
+void make_tensor_map_3d(CUtensorMap *map, const void *base, uint64_t dim0, uint64_t dim1, uint64_t dim2,
+                        uint32_t box0, uint32_t box1) {
+    using Encode = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static Encode encode = nullptr;
+    if (!encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        UPDC_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (!fn || q != cudaDriverEntryPointSuccess) throw Error(-2, "cuTensorMapEncodeTiled is unavailable");
+        encode = (Encode)fn;
+    }
+    // the layout rules of tiled TMA copies, checked before the driver sees them
+    if (((uintptr_t)base & 15) || (dim0 * 8) % 16 || (box0 * 8) % 16 || box0 > 256 || box1 > 256 || box0 > dim0)
+        throw Error(-2, "tensor map layout violates TMA alignment rules");
+    const cuuint64_t dims[3] = {dim0, dim1, dim2};
+    const cuuint64_t strides[2] = {dim0 * 8, dim0 * dim1 * 8};
+    const cuuint32_t box[3] = {box0, box1, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void *>(base), dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error(-2, "cuTensorMapEncodeTiled failed with status " + std::to_string((int)r));
+}
+
 const char *error_message(uint32_t code) {
     switch (code) {
         case ERR_NONFINITE_MEAN: return "non-finite forward mean";
@@ -26,6 +52,7 @@ const char *error_message(uint32_t code) {
         case ERR_NONFINITE_INITIAL: return "non-finite signed initial estimate";
         case ERR_INVALID_PSF_PIXEL: return "invalid PSF pixel";
         case ERR_LINKMAP_TARGET: return "invalid or obsolete LinkMap cache";
+        case ERR_DEVICE_TIMEOUT: return "device wait timed out";
         default: return "unknown device error";
     }
 }
@@ -42,20 +69,30 @@ int next_smooth(int n, bool even) {
     }
 }
 
-bool fft_factor(int n, std::vector<int> &radices) {
+bool fft_factor(int n, int rmax, std::vector<int> &radices) {
+    // candidate radices in the order the device stage loops run them
+    static const int order[] = {32, 28, 27, 25, 24, 21, 20, 18, 16, 15, 14, 12, 10, 9, 8, 7, 6, 5, 4, 3, 2};
     radices.clear();
     int m = n;
-    while (m % 8 == 0) { radices.push_back(8); m /= 8; }
-    while (m % 4 == 0) { radices.push_back(4); m /= 4; }
-    while (m % 2 == 0) { radices.push_back(2); m /= 2; }
-    for (int r : {7, 5, 3})
-        while (m % r == 0) { radices.push_back(r); m /= r; }
-    return m == 1 && (int)radices.size() <= FFT_MAX_STAGES;
+    while (m > 1) {
+        int pick = 0;
+        for (int r : order)
+            if (r <= rmax && m % r == 0) { pick = r; break; }
+        if (!pick) return false;
+        radices.push_back(pick);
+        m /= pick;
+    }
+    std::vector<int> sorted;
+    for (int r : order)
+        for (int x : radices)
+            if (x == r) sorted.push_back(x);
+    radices = sorted;
+    return (int)radices.size() <= FFT_MAX_STAGES;
 }
 
-template <typename T> std::vector<cx<T>> fft_make_table(int n, FftPlan &plan) {
+template <typename T> std::vector<cx<T>> fft_make_table(int n, int rmax, FftPlan &plan) {
     std::vector<int> rad;
-    if (!fft_factor(n, rad)) throw Error(1, "FFT length " + std::to_string(n) + " is not 7-smooth");
+    if (!fft_factor(n, rmax, rad)) throw Error(1, "FFT length " + std::to_string(n) + " is not 7-smooth");
     std::vector<cx<T>> tab;
     plan.n = n;
     plan.nstage = (int)rad.size();
@@ -78,8 +115,78 @@ template <typename T> std::vector<cx<T>> fft_make_table(int n, FftPlan &plan) {
     if (tab.empty()) tab.push_back(cx<T>{1, 0});
     return tab;
 }
-template std::vector<cx<float>> fft_make_table<float>(int, FftPlan &);
-template std::vector<cx<double>> fft_make_table<double>(int, FftPlan &);
+template std::vector<cx<float>> fft_make_table<float>(int, int, FftPlan &);
+template std::vector<cx<double>> fft_make_table<double>(int, int, FftPlan &);
+
+namespace {
+// Output slot of register p in the codelet of radix R (Dft<R>::out).
+int codelet_out(int R, int p) {
+    static const int split[][3] = {{6, 2, 3}, {9, 3, 3}, {10, 2, 5}, {12, 4, 3}, {14, 2, 7}, {15, 3, 5}, {16, 4, 4},
+                                   {18, 2, 9}, {20, 4, 5}, {21, 3, 7}, {24, 8, 3}, {25, 5, 5}, {27, 3, 9}, {28, 4, 7},
+                                   {32, 4, 8}};
+    for (const auto &sp : split)
+        if (sp[0] == R) return p / sp[2] + sp[1] * codelet_out(sp[2], p % sp[2]);
+    return p;
+}
+// Shared-memory wavefronts of one warp access of 8-byte elements: two
+// half-warp phases, each costing the largest number of distinct addresses in
+// one bank pair.
+int warp_wavefronts(const int *addr, int shift) {
+    int total = 0;
+    for (int h = 0; h < 2; ++h) {
+        int slots[16][16];
+        int cnt[16] = {0};
+        for (int l = 16 * h; l < 16 * h + 16; ++l) {
+            if (addr[l] < 0) continue;
+            const int a = fpad(addr[l], shift), b = a & 15;
+            bool seen = false;
+            for (int i = 0; i < cnt[b]; ++i) seen |= slots[b][i] == a;
+            if (!seen) slots[b][cnt[b]++] = a;
+        }
+        int mx = 0;
+        for (int b = 0; b < 16; ++b) mx = std::max(mx, cnt[b]);
+        total += mx;
+    }
+    return total;
+}
+}  // namespace
+
+int fft_choose_padding(const FftPlan &plan, int nt, int cap, int batch) {
+    int best_shift = 31;
+    long best = -1;
+    for (int shift : {31, 5, 4}) {
+        long cost = 0;
+        const int n = plan.n;
+        for (int s = 0; s < plan.nstage; ++s) {
+            const int R = plan.radix[s], Ns = plan.ns[s], nb = n / R, total = nb * batch;
+            const int K = (cap / R + nt - 1) / nt;
+            int addr[32];
+            for (int kk = 0; kk < K; ++kk)
+                for (int w = 0; w < nt / 32; ++w) {
+                    if (w * 32 + kk * nt >= total) break;
+                    for (int r = 0; r < R; ++r) {
+                        for (int l = 0; l < 32; ++l) {
+                            const int b = w * 32 + l + kk * nt;
+                            addr[l] = b < total ? (b / nb) * n + b % nb + r * nb : -1;
+                        }
+                        cost += warp_wavefronts(addr, shift);
+                        for (int l = 0; l < 32; ++l) {
+                            const int b = w * 32 + l + kk * nt;
+                            if (b >= total) { addr[l] = -1; continue; }
+                            const int row = b / nb, j = b % nb, k = j % Ns;
+                            addr[l] = row * n + (j - k) * R + k + codelet_out(R, r) * Ns;
+                        }
+                        cost += warp_wavefronts(addr, shift);
+                    }
+                }
+        }
+        if (best < 0 || cost < best) {
+            best = cost;
+            best_shift = shift;
+        }
+    }
+    return best_shift;
+}
 
 namespace {
 
@@ -326,9 +433,9 @@ template <typename T> class EngineImpl final : public Engine {
     void stage_forward(int k) override {
         (void)k;
         reset_iteration_state();
-        launch_row_r2c_plane(estimate_, rx_, 1, 0, 0);
+        launch_row_r2c_plane(estimate_, rx_, 1, 0, map_rx_);
         launch_col_forward();
-        launch_row_c2r_batched(y_, nexp_, blur_);
+        launch_row_c2r_batched(y_, nexp_, blur_, map_y_);
         UPDC_CUDA(cudaStreamSynchronize(stream_));
     }
     void stage_detector(int k, IterationRecord *rec) override {
@@ -350,9 +457,9 @@ template <typename T> class EngineImpl final : public Engine {
         (void)k;
     }
     void stage_correction() override {
-        launch_row_r2c_plane(scatter_, rs_, nexp_, nout_, (size_t)(M_ + 1) * H_);
+        launch_row_r2c_plane(scatter_, rs_, nexp_, nout_, map_rs_);
         launch_col_adjoint();
-        launch_row_c2r_batched(cr_, 1, correction_);
+        launch_row_c2r_batched(cr_, 1, correction_, map_cr_);
         UPDC_CUDA(cudaStreamSynchronize(stream_));
     }
     void stage_update(IterationRecord *rec) override {
@@ -463,8 +570,10 @@ template <typename T> class EngineImpl final : public Engine {
         if (M_ > Caps<T>::ROW) throw Error(1, "FFT width exceeds the row-transform capacity");
         if (FH_ > Caps<T>::COL_L) throw Error(1, "FFT height exceeds the column-transform capacity");
         // twiddle tables
-        auto tm = fft_make_table<T>(M_, plan_m_);
-        auto th = fft_make_table<T>(FH_, plan_h_);
+        auto tm = fft_make_table<T>(M_, FFT_RMAX, plan_m_);
+        auto th = fft_make_table<T>(FH_, FFT_RMAX, plan_h_);
+        plan_m_.pad_shift = fft_choose_padding(plan_m_, NT, Caps<T>::ROW, std::max(1, std::min(2, Caps<T>::ROW / M_)));
+        plan_h_.pad_shift = fft_choose_padding(plan_h_, NT, Caps<T>::COL_S, 1);
         cx<T> *dm = alloc<cx<T>>(tm.size()), *dh = alloc<cx<T>>(th.size());
         UPDC_CUDA(cudaMemcpy(dm, tm.data(), tm.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
         UPDC_CUDA(cudaMemcpy(dh, th.data(), th.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
@@ -481,6 +590,9 @@ template <typename T> class EngineImpl final : public Engine {
 
     void allocate() {
         const size_t nu = (size_t)M_ + 1;
+        // u-major spectra keep H rows at an even pitch for FP32 so that every
+        // u-row starts on a 16-byte boundary (TMA strides are multiples of 16)
+        ldh_ = sizeof(T) == 4 ? (H_ + 1) & ~1 : H_;
         estimate_ = alloc<T>(nout_);
         coverage_ = alloc<T>(nout_);
         den_ = alloc<T>(nout_);
@@ -492,10 +604,12 @@ template <typename T> class EngineImpl final : public Engine {
         wht_ = alloc<T>(nexp_ * nin_);
         frozen_ = alloc<uint8_t>(nexp_ * nin_);
         UPDC_CUDA(cudaMemset(frozen_, 0, nexp_ * nin_));
-        rx_ = alloc<cx<T>>(nu * H_);
-        cr_ = alloc<cx<T>>(nu * H_);
-        y_ = alloc<cx<T>>(nexp_ * nu * H_);
-        rs_ = alloc<cx<T>>(nexp_ * nu * H_);
+        rx_ = alloc<cx<T>>(nu * ldh_);
+        cr_ = alloc<cx<T>>(nu * ldh_);
+        y_ = alloc<cx<T>>(nexp_ * nu * ldh_);
+        rs_ = alloc<cx<T>>(nexp_ * nu * ldh_);
+        for (auto *p : {rx_, cr_}) UPDC_CUDA(cudaMemset(p, 0, nu * ldh_ * sizeof(cx<T>)));
+        for (auto *p : {y_, rs_}) UPDC_CUDA(cudaMemset(p, 0, nexp_ * nu * ldh_ * sizeof(cx<T>)));
         khat_ = alloc<cx<T>>(nexp_ * nu * FH_);
         d_exps_ = alloc<ExpDesc<T>>(nexp_);
         d_stats_ = alloc<ExpStats>(nexp_);
@@ -505,34 +619,60 @@ template <typename T> class EngineImpl final : public Engine {
         d_part_neg_ = alloc<unsigned long long>(upd_grid_);
         d_red_sum_ = alloc<double>(1);
         d_red_neg_ = alloc<unsigned long long>(1);
-        if (2 * align16((size_t)FH_ * sizeof(cx<T>)) > SMEM_LIMIT) aux_fwd_ = alloc<cx<T>>(nu * FH_);
+        if (fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift) + align16((size_t)FH_ * sizeof(cx<T>)) > SMEM_LIMIT) aux_fwd_ = alloc<cx<T>>(nu * FH_);
         links_.assign(nexp_, DevLinkMap());
-        // kernel attributes
+        // rows per row-transform block; the TMA path needs an even number of
+        // 8-byte elements per row tile (16-byte box rows and coordinates)
+        constexpr int EW = TmaElems<T>::value;
+        row_b_ = std::max(1, std::min({Caps<T>::ROW / M_, TMA_UBOX / EW, ldh_}));
+        if (EW == 1 && row_b_ >= 2) row_b_ &= ~1;
+        // the FFT buffer and the staging tile share the block's shared memory
+        while (row_b_ > 2 && row_buf_bytes(row_b_, M_, sizeof(cx<T>), plan_m_.pad_shift) + row_stage_bytes(row_b_, M_, sizeof(cx<T>)) > SMEM_LIMIT)
+            row_b_ -= EW == 1 ? 2 : 1;
+        use_tma_ = (row_b_ * EW) % 2 == 0 &&
+                   row_buf_bytes(row_b_, M_, sizeof(cx<T>), plan_m_.pad_shift) + row_stage_bytes(row_b_, M_, sizeof(cx<T>)) <= SMEM_LIMIT;
+        if (use_tma_) {
+            const uint64_t d0 = (uint64_t)ldh_ * EW;
+            const uint32_t ub = (uint32_t)row_ubox(M_);
+            make_tensor_map_3d(&map_rx_, rx_, d0, nu, 1, row_b_ * EW, ub);
+            make_tensor_map_3d(&map_cr_, cr_, d0, nu, 1, row_b_ * EW, ub);
+            make_tensor_map_3d(&map_y_, y_, d0, nu, nexp_, row_b_ * EW, ub);
+            make_tensor_map_3d(&map_rs_, rs_, d0, nu, nexp_, row_b_ * EW, ub);
+        }
         configure_kernels();
     }
 
     // ------------------------------------------------------------------ kernel configuration
-    size_t row_smem() const { return (size_t)(Caps<T>::ROW / M_) * M_ * sizeof(cx<T>); }
-    int row_batch() const { return Caps<T>::ROW / M_; }
-    size_t fwd_smem() const { return aux_fwd_ ? align16(FH_ * sizeof(cx<T>)) : 2 * align16(FH_ * sizeof(cx<T>)); }
+    int ldh_ = 0, row_b_ = 1;
+    bool use_tma_ = false;
+    CUtensorMap map_rx_{}, map_cr_{}, map_y_{}, map_rs_{}, no_map_{};
+
+    size_t row_smem() const {
+        return row_buf_bytes(row_b_, M_, sizeof(cx<T>), plan_m_.pad_shift) + (use_tma_ ? row_stage_bytes(row_b_, M_, sizeof(cx<T>)) : 0);
+    }
+    int row_batch() const { return row_b_; }
+    size_t fwd_smem() const {
+        return fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift) + (aux_fwd_ ? 0 : align16(FH_ * sizeof(cx<T>)));
+    }
     template <class Acc> size_t adj_smem() const {
-        const size_t b = align16(FH_ * sizeof(cx<T>)) + align16(FH_ * sizeof(typename Acc::S));
-        return b > SMEM_LIMIT ? align16(FH_ * sizeof(cx<T>)) : b;
+        const size_t b = fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift) + align16(FH_ * sizeof(typename Acc::S));
+        return b > SMEM_LIMIT ? fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift) : b;
     }
     template <class Acc> bool adj_aux() const {
-        return align16(FH_ * sizeof(cx<T>)) + align16(FH_ * sizeof(typename Acc::S)) > SMEM_LIMIT;
+        return fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift) + align16(FH_ * sizeof(typename Acc::S)) > SMEM_LIMIT;
     }
 
     void configure_kernels() {
         const size_t rs = row_smem();
-        set_smem(k_row_r2c<T, NT, Caps<T>::ROW, PlaneLoader<T>>, rs);
-        set_smem(k_row_r2c<T, NT, Caps<T>::ROW, PsfLoader<T>>, rs);
-        set_smem(k_row_c2r<T, NT, Caps<T>::ROW, PlaneStore<T>>, rs);
+        set_smem(k_row_r2c<T, NT, Caps<T>::ROW, PlaneLoader<T>, true>, rs);
+        set_smem(k_row_r2c<T, NT, Caps<T>::ROW, PlaneLoader<T>, false>, rs);
+        set_smem(k_row_c2r<T, NT, Caps<T>::ROW, PlaneStore<T>, true>, rs);
+        set_smem(k_row_c2r<T, NT, Caps<T>::ROW, PlaneStore<T>, false>, rs);
         const size_t fs = fwd_smem();
         set_smem(k_col_forward<T, NT, Caps<T>::COL_S>, fs);
         set_smem(k_col_forward<T, NT, Caps<T>::COL_L>, fs);
-        set_smem(k_col_fft<T, NT, Caps<T>::COL_S, false>, align16(FH_ * sizeof(cx<T>)));
-        set_smem(k_col_fft<T, NT, Caps<T>::COL_L, false>, align16(FH_ * sizeof(cx<T>)));
+        set_smem(k_col_fft<T, NT, Caps<T>::COL_S, false>, fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift));
+        set_smem(k_col_fft<T, NT, Caps<T>::COL_L, false>, fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift));
         configure_adjoint<AccPlain<T>>();
         if (sizeof(T) == 4) {
             configure_adjoint<AccF64>();
@@ -543,36 +683,34 @@ template <typename T> class EngineImpl final : public Engine {
         if constexpr (sizeof(typename Acc::S) > 0) {
             if constexpr (std::is_same<Acc, AccPlain<T>>::value || sizeof(T) == 4) {
                 const size_t s = adj_smem<Acc>();
-                set_smem(k_col_adjoint<T, Acc, NtAdj<T>::value,Caps<T>::COL_S>, s);
-                set_smem(k_col_adjoint<T, Acc, NtAdj<T>::value,Caps<T>::COL_L>, s);
+                set_smem(k_col_adjoint<T, Acc, NtAdj<T>::value, Caps<T>::COL_S>, s);
+                set_smem(k_col_adjoint<T, Acc, NtAdj<T>::value, Caps<T>::COL_L>, s);
             }
         }
     }
 
     // ------------------------------------------------------------------ launches
-    template <class Loader>
-    void launch_row_r2c(const Loader &ld, int rows, int batch, cx<T> *out, int ldo, size_t out_stride) {
+    // planes [batch][H][W] -> u-major spectra [batch][M+1][ldh], one launch
+    void launch_row_r2c_plane(const T *plane, cx<T> *out, int batch, size_t plane_stride, const CUtensorMap &map) {
         const int B = row_batch();
-        dim3 grid((unsigned)ceil_div(rows, B), (unsigned)batch);
-        k_row_r2c<T, NT, Caps<T>::ROW, Loader><<<grid, NT, row_smem(), stream_>>>(d_plan_m_, post_, ld, W_, rows, B, out, ldo, out_stride);
+        dim3 grid((unsigned)ceil_div(H_, B), (unsigned)batch);
+        const PlaneLoader<T> ld{plane, W_, plane_stride};
+        const SpecRef ref{out, ldh_, (size_t)(M_ + 1) * ldh_};
+        if (use_tma_)
+            k_row_r2c<T, NT, Caps<T>::ROW, PlaneLoader<T>, true><<<grid, NT, row_smem(), stream_>>>(
+                d_plan_m_, post_, ld, W_, H_, B, ref, map);
+        else
+            k_row_r2c<T, NT, Caps<T>::ROW, PlaneLoader<T>, false><<<grid, NT, row_smem(), stream_>>>(
+                d_plan_m_, post_, ld, W_, H_, B, ref, no_map_);
         UPDC_CUDA(cudaGetLastError());
-    }
-    // planes [batch][H][W] -> u-major [batch][M+1][H]
-    void launch_row_r2c_plane(const T *plane, cx<T> *out, int batch, size_t plane_stride, size_t out_stride) {
-        if (batch == 1) {
-            launch_row_r2c(PlaneLoader<T>{plane, W_}, H_, 1, out, H_, 0);
-            return;
-        }
-        for (int k = 0; k < batch; ++k)
-            launch_row_r2c(PlaneLoader<T>{plane + k * plane_stride, W_}, H_, 1, out + k * out_stride, H_, 0);
     }
     void launch_col_forward() {
         const size_t nu = (size_t)M_ + 1;
-        const size_t ks = nu * FH_, ys = nu * H_;
+        const size_t ks = nu * FH_, ys = nu * ldh_;
         if (FH_ <= Caps<T>::COL_S)
-            k_col_forward<T, NT, Caps<T>::COL_S><<<(unsigned)nu, NT, fwd_smem(), stream_>>>(d_plan_h_, rx_, H_, H_, khat_, ks, nexp_, y_, H_, ys, H_, (int)nu, aux_fwd_);
+            k_col_forward<T, NT, Caps<T>::COL_S><<<(unsigned)nu, NT, fwd_smem(), stream_>>>(d_plan_h_, rx_, ldh_, H_, khat_, ks, nexp_, y_, ldh_, ys, H_, (int)nu, aux_fwd_);
         else
-            k_col_forward<T, NT, Caps<T>::COL_L><<<(unsigned)nu, NT, fwd_smem(), stream_>>>(d_plan_h_, rx_, H_, H_, khat_, ks, nexp_, y_, H_, ys, H_, (int)nu, aux_fwd_);
+            k_col_forward<T, NT, Caps<T>::COL_L><<<(unsigned)nu, NT, fwd_smem(), stream_>>>(d_plan_h_, rx_, ldh_, H_, khat_, ks, nexp_, y_, ldh_, ys, H_, (int)nu, aux_fwd_);
         UPDC_CUDA(cudaGetLastError());
     }
     template <class Acc> void launch_col_adjoint_t(const cx<T> *khat) {
@@ -584,9 +722,9 @@ template <typename T> class EngineImpl final : public Engine {
         }
         const size_t s = adj_smem<Acc>();
         if (FH_ <= Caps<T>::COL_S)
-            k_col_adjoint<T, Acc, NtAdj<T>::value,Caps<T>::COL_S><<<(unsigned)nu, NtAdj<T>::value, s, stream_>>>(d_plan_h_, rs_, H_, nu * H_, H_, khat, nu * FH_, nexp_, cr_, H_, H_, aux);
+            k_col_adjoint<T, Acc, NtAdj<T>::value, Caps<T>::COL_S><<<(unsigned)nu, NtAdj<T>::value, s, stream_>>>(d_plan_h_, rs_, ldh_, nu * ldh_, H_, khat, nu * FH_, nexp_, cr_, ldh_, H_, aux);
         else
-            k_col_adjoint<T, Acc, NtAdj<T>::value,Caps<T>::COL_L><<<(unsigned)nu, NtAdj<T>::value, s, stream_>>>(d_plan_h_, rs_, H_, nu * H_, H_, khat, nu * FH_, nexp_, cr_, H_, H_, aux);
+            k_col_adjoint<T, Acc, NtAdj<T>::value, Caps<T>::COL_L><<<(unsigned)nu, NtAdj<T>::value, s, stream_>>>(d_plan_h_, rs_, ldh_, nu * ldh_, H_, khat, nu * FH_, nexp_, cr_, ldh_, H_, aux);
         UPDC_CUDA(cudaGetLastError());
     }
     void launch_col_adjoint() {
@@ -596,12 +734,17 @@ template <typename T> class EngineImpl final : public Engine {
         }
         launch_col_adjoint_t<AccPlain<T>>(khat_);
     }
-    void launch_row_c2r_batched(const cx<T> *in, int batch, T *out) {
+    void launch_row_c2r_batched(const cx<T> *in, int batch, T *out, const CUtensorMap &map) {
         const int B = row_batch();
         dim3 grid((unsigned)ceil_div(H_, B), (unsigned)batch);
         const T scale = scale_factor();
-        k_row_c2r<T, NT, Caps<T>::ROW, PlaneStore<T>><<<grid, NT, row_smem(), stream_>>>(
-            d_plan_m_, post_, in, H_, (size_t)(M_ + 1) * H_, H_, W_, B, scale, PlaneStore<T>{out, W_, nout_});
+        const SpecRef ref{const_cast<cx<T> *>(in), ldh_, (size_t)(M_ + 1) * ldh_};
+        if (use_tma_)
+            k_row_c2r<T, NT, Caps<T>::ROW, PlaneStore<T>, true><<<grid, NT, row_smem(), stream_>>>(
+                d_plan_m_, post_, ref, map, H_, W_, B, scale, PlaneStore<T>{out, W_, nout_}, d_err_);
+        else
+            k_row_c2r<T, NT, Caps<T>::ROW, PlaneStore<T>, false><<<grid, NT, row_smem(), stream_>>>(
+                d_plan_m_, post_, ref, no_map_, H_, W_, B, scale, PlaneStore<T>{out, W_, nout_}, d_err_);
         UPDC_CUDA(cudaGetLastError());
     }
     T scale_factor() const {
@@ -646,20 +789,20 @@ template <typename T> class EngineImpl final : public Engine {
             UPDC_CUDA(cudaEventRecord(ev[0], stream_));
         }
         reset_iteration_state();
-        launch_row_r2c_plane(estimate_, rx_, 1, 0, 0);                      // estimate R2C, x pass
+        launch_row_r2c_plane(estimate_, rx_, 1, 0, map_rx_);                      // estimate R2C, x pass
         if (timed) UPDC_CUDA(cudaEventRecord(ev[1], stream_));
         launch_col_forward();                                               // y pass + OTF + inverse y pass
         if (timed) UPDC_CUDA(cudaEventRecord(ev[2], stream_));
-        launch_row_c2r_batched(y_, nexp_, blur_);                           // inverse x pass + crop
+        launch_row_c2r_batched(y_, nexp_, blur_, map_y_);                           // inverse x pass + crop
         if (timed) UPDC_CUDA(cudaEventRecord(ev[3], stream_));
         launch_detector();                                                  // gather / FreezeMu / ratio
         if (timed) UPDC_CUDA(cudaEventRecord(ev[4], stream_));
         launch_scatter(wr_, scatter_);                                      // S^T (transposed gather)
         if (timed) UPDC_CUDA(cudaEventRecord(ev[5], stream_));
-        launch_row_r2c_plane(scatter_, rs_, nexp_, nout_, (size_t)(M_ + 1) * H_);  // scatter R2C, x pass
+        launch_row_r2c_plane(scatter_, rs_, nexp_, nout_, map_rs_);  // scatter R2C, x pass
         if (timed) UPDC_CUDA(cudaEventRecord(ev[6], stream_));
         launch_col_adjoint();                                               // y pass, conj-OTF sum, inverse y
-        launch_row_c2r_batched(cr_, 1, correction_);                        // inverse x pass + crop
+        launch_row_c2r_batched(cr_, 1, correction_, map_cr_);                        // inverse x pass + crop
         if (timed) UPDC_CUDA(cudaEventRecord(ev[7], stream_));
         launch_update();
         if (timed) {
@@ -819,7 +962,9 @@ template <typename T> class EngineImpl final : public Engine {
     }
 
     // PSF spectra K_k (u-major, (M+1) x FH) of precision U into dst.
-    template <typename U> void psf_spectra(cx<U> *dst, bool fp64_sum, const FftPlan *pm, const FftPlan *ph, const cx<U> *post) {
+    template <typename U>
+    void psf_spectra(cx<U> *dst, bool fp64_sum, const FftPlan *pm, const FftPlan *ph, const FftPlan &hpm, const FftPlan &hph,
+                     const cx<U> *post) {
         const size_t nu = (size_t)M_ + 1;
         cx<U> *rp = dalloc<cx<U>>(nu * FH_, nullptr);
         for (int k = 0; k < nexp_; ++k) {
@@ -857,11 +1002,12 @@ template <typename T> class EngineImpl final : public Engine {
             PsfLoader<U> ld{dp, e.psf_width, transposed_ ? e.psf_height : e.psf_width,
                             transposed_ ? e.psf_width : e.psf_height, FW_, FH_, transposed_, inv};
             const int B = Caps<U>::ROW / M_;
-            const size_t rsm = (size_t)B * M_ * sizeof(cx<U>);
-            set_smem(k_row_r2c<U, NT, Caps<U>::ROW, PsfLoader<U>>, rsm);
+            const size_t rsm = row_buf_bytes(B, M_, sizeof(cx<U>), hpm.pad_shift);
+            set_smem(k_row_r2c<U, NT, Caps<U>::ROW, PsfLoader<U>, false>, rsm);
             dim3 grid((unsigned)ceil_div(FH_, B), 1);
-            k_row_r2c<U, NT, Caps<U>::ROW, PsfLoader<U>><<<grid, NT, rsm, stream_>>>(pm, post, ld, FW_, FH_, B, rp, FH_, 0);
-            const size_t cs = align16(FH_ * sizeof(cx<U>));
+            k_row_r2c<U, NT, Caps<U>::ROW, PsfLoader<U>, false><<<grid, NT, rsm, stream_>>>(
+                pm, post, ld, FW_, FH_, B, SpecRef{rp, FH_, 0}, no_map_);
+            const size_t cs = fft_buf_bytes(FH_, sizeof(cx<U>), hph.pad_shift);
             cx<U> *out = dst + (size_t)k * nu * FH_;
             if (FH_ <= Caps<U>::COL_S) {
                 set_smem(k_col_fft<U, NT, Caps<U>::COL_S, false>, cs);
@@ -879,7 +1025,7 @@ template <typename T> class EngineImpl final : public Engine {
 
     void prepare_psf_spectra() {
         const bool fp64_sum = opt_.form == FORM_FP32 || opt_.form == FORM_FP64;
-        psf_spectra<T>(khat_, fp64_sum, d_plan_m_, d_plan_h_, post_);
+        psf_spectra<T>(khat_, fp64_sum, d_plan_m_, d_plan_h_, plan_m_, plan_h_, post_);
     }
 
     void drizzle() {
@@ -896,9 +1042,9 @@ template <typename T> class EngineImpl final : public Engine {
         else {
             dim3 grid((unsigned)std::min<size_t>(ceil_div(nout_, 256), 148 * 8), (unsigned)nexp_);
             k_scatter_t<T, T, T><<<grid, 256, 0, stream_>>>(d_exps_, nin_, nout_, (const T *)nullptr, 1, scatter_);
-            launch_row_r2c_plane(scatter_, rs_, nexp_, nout_, (size_t)(M_ + 1) * H_);
+            launch_row_r2c_plane(scatter_, rs_, nexp_, nout_, map_rs_);
             launch_col_adjoint();
-            launch_row_c2r_batched(cr_, 1, den_);
+            launch_row_c2r_batched(cr_, 1, den_, map_cr_);
         }
         finish_denominator();
     }
@@ -908,8 +1054,10 @@ template <typename T> class EngineImpl final : public Engine {
         using D = double;
         const size_t nu = (size_t)M_ + 1;
         FftPlan pm, ph;
-        auto tm = fft_make_table<D>(M_, pm);
-        auto th = fft_make_table<D>(FH_, ph);
+        auto tm = fft_make_table<D>(M_, FFT_RMAX, pm);
+        auto th = fft_make_table<D>(FH_, FFT_RMAX, ph);
+        pm.pad_shift = fft_choose_padding(pm, NT, Caps<D>::ROW, std::max(1, std::min(2, Caps<D>::ROW / M_)));
+        ph.pad_shift = fft_choose_padding(ph, NtAdj<D>::value, Caps<D>::COL_S, 1);
         cx<D> *dm = dalloc<cx<D>>(tm.size(), nullptr), *dh = dalloc<cx<D>>(th.size(), nullptr);
         UPDC_CUDA(cudaMemcpy(dm, tm.data(), tm.size() * sizeof(cx<D>), cudaMemcpyHostToDevice));
         UPDC_CUDA(cudaMemcpy(dh, th.data(), th.size() * sizeof(cx<D>), cudaMemcpyHostToDevice));
@@ -924,22 +1072,23 @@ template <typename T> class EngineImpl final : public Engine {
         cx<D> *dpost = dalloc<cx<D>>(M_ + 1, nullptr);
         UPDC_CUDA(cudaMemcpy(dpost, post.data(), post.size() * sizeof(cx<D>), cudaMemcpyHostToDevice));
         cx<D> *kd = dalloc<cx<D>>(nexp_ * nu * FH_, nullptr);
-        psf_spectra<D>(kd, true, dpm, dph, dpost);
+        psf_spectra<D>(kd, true, dpm, dph, pm, ph, dpost);
         D *sc = dalloc<D>(nexp_ * nout_, nullptr);
         dim3 grid((unsigned)std::min<size_t>(ceil_div(nout_, 256), 148 * 8), (unsigned)nexp_);
         k_scatter_t<T, D, T><<<grid, 256, 0, stream_>>>(d_exps_, nin_, nout_, (const T *)nullptr, 1, sc);
         cx<D> *rs = dalloc<cx<D>>(nexp_ * nu * H_, nullptr), *cr = dalloc<cx<D>>(nu * H_, nullptr);
         const int B = Caps<D>::ROW / M_;
-        const size_t rsm = (size_t)B * M_ * sizeof(cx<D>);
-        set_smem(k_row_r2c<D, NT, Caps<D>::ROW, PlaneLoader<D>>, rsm);
-        for (int k = 0; k < nexp_; ++k) {
-            dim3 g((unsigned)ceil_div(H_, B), 1);
-            k_row_r2c<D, NT, Caps<D>::ROW, PlaneLoader<D>><<<g, NT, rsm, stream_>>>(dpm, dpost, PlaneLoader<D>{sc + k * nout_, W_}, W_, H_, B, rs + k * nu * H_, H_, 0);
+        const size_t rsm = row_buf_bytes(B, M_, sizeof(cx<D>), pm.pad_shift);
+        set_smem(k_row_r2c<D, NT, Caps<D>::ROW, PlaneLoader<D>, false>, rsm);
+        {
+            dim3 g((unsigned)ceil_div(H_, B), (unsigned)nexp_);
+            k_row_r2c<D, NT, Caps<D>::ROW, PlaneLoader<D>, false><<<g, NT, rsm, stream_>>>(
+                dpm, dpost, PlaneLoader<D>{sc, W_, nout_}, W_, H_, B, SpecRef{rs, H_, nu * H_}, no_map_);
         }
-        const size_t b = align16(FH_ * sizeof(cx<D>));
-        const bool aux_needed = 2 * b > SMEM_LIMIT;
+        const size_t b = fft_buf_bytes(FH_, sizeof(cx<D>), ph.pad_shift);
+        const bool aux_needed = b + align16(FH_ * sizeof(cx<D>)) > SMEM_LIMIT;
         cx<D> *aux = aux_needed ? dalloc<cx<D>>(nu * FH_, nullptr) : nullptr;
-        const size_t s = aux_needed ? b : 2 * b;
+        const size_t s = aux_needed ? b : b + align16(FH_ * sizeof(cx<D>));
         if (FH_ <= Caps<D>::COL_S) {
             set_smem(k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_S>, s);
             k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_S><<<(unsigned)nu, NtAdj<D>::value, s, stream_>>>(dph, rs, H_, nu * H_, H_, kd, nu * FH_, nexp_, cr, H_, H_, aux);
@@ -948,10 +1097,11 @@ template <typename T> class EngineImpl final : public Engine {
             k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_L><<<(unsigned)nu, NtAdj<D>::value, s, stream_>>>(dph, rs, H_, nu * H_, H_, kd, nu * FH_, nexp_, cr, H_, H_, aux);
         }
         D *den = dalloc<D>(nout_, nullptr);
-        set_smem(k_row_c2r<D, NT, Caps<D>::ROW, PlaneStore<D>>, rsm);
+        set_smem(k_row_c2r<D, NT, Caps<D>::ROW, PlaneStore<D>, false>, rsm);
         dim3 g2((unsigned)ceil_div(H_, B), 1);
-        k_row_c2r<D, NT, Caps<D>::ROW, PlaneStore<D>><<<g2, NT, rsm, stream_>>>(dpm, dpost, cr, H_, 0, H_, W_, B,
-                                                                                1.0 / (double)((size_t)FW_ * FH_), PlaneStore<D>{den, W_, 0});
+        k_row_c2r<D, NT, Caps<D>::ROW, PlaneStore<D>, false><<<g2, NT, rsm, stream_>>>(
+            dpm, dpost, SpecRef{cr, H_, 0}, no_map_, H_, W_, B, 1.0 / (double)((size_t)FW_ * FH_),
+            PlaneStore<D>{den, W_, 0}, d_err_);
         k_convert<D, T><<<grid1d(nout_), 256, 0, stream_>>>(den, den_, nout_);
         UPDC_CUDA(cudaGetLastError());
         UPDC_CUDA(cudaStreamSynchronize(stream_));

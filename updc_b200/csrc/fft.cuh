@@ -8,8 +8,17 @@
 // (self-sorting Stockham).  All loads of a stage are staged in registers
 // before a barrier and all stores follow it, so one buffer suffices.
 // Twiddles come from a table computed in double precision on the host.
+//
+// Radices are 2, 3, 4, 5, 7, 8 and composites R = A*B (up to 32) computed in
+// registers as A-point DFTs, internal twiddles, then B-point DFTs; composites
+// leave their outputs in a compile-time permuted register order that the
+// stage's store phase undoes, so no extra registers are needed.  Fewer,
+// larger stages mean fewer shared-memory passes and barriers.  The shared
+// buffer is padded by one element every 32 (fpad) so the strided stores of
+// early stages do not pile onto one bank.
 #pragma once
 
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -46,16 +55,28 @@ struct FftPlan {
     int twoff[FFT_MAX_STAGES] = {};
     FastDiv ns_div[FFT_MAX_STAGES];   // division by Ns
     FastDiv nb_div[FFT_MAX_STAGES];   // division by n / radix
+    int pad_shift = 31;               // shared-memory padding: one slot every 2^pad_shift elements
     const void *tw = nullptr;  // device table of cx<T>, forward sign
 };
 
-// Radix order: 8s first, then 4, 2, 7, 5, 3.  Returns false when n has a
-// prime factor above 7.
-bool fft_factor(int n, std::vector<int> &radices);
+// Splits n into radices no larger than rmax (greedy, largest first), ordered
+// as the device stage loops run them (descending).  Returns false when n has
+// a prime factor above 7.
+bool fft_factor(int n, int rmax, std::vector<int> &radices);
+
+// Padded shared-memory index of logical element e: one pad slot every
+// 2^shift elements (shift 31: no padding).  The plan's shift is chosen on the
+// host by simulating the bank pattern of its stages (fft_choose_padding).
+__host__ __device__ __forceinline__ int fpad(int e, int shift) { return e + (e >> shift); }
+// Shared-memory elements for `count` logical elements.
+__host__ __device__ __forceinline__ int fpad_size(int count, int shift) { return count + (count >> shift) + 1; }
+// Picks the padding shift with the fewest simulated shared-memory wavefronts
+// for the plan's stages (8-byte elements, NT threads, batch transforms).
+int fft_choose_padding(const FftPlan &plan, int nt, int cap, int batch);
 
 // Builds the host twiddle table for n (complex, forward sign) and fills the
 // plan's stage fields.  The caller uploads the table and sets plan.tw.
-template <typename T> std::vector<cx<T>> fft_make_table(int n, FftPlan &plan);
+template <typename T> std::vector<cx<T>> fft_make_table(int n, int rmax, FftPlan &plan);
 
 // ----------------------------------------------------------------------------- DFT kernels
 template <typename T> struct DftConst;
@@ -79,21 +100,23 @@ template <> struct DftConst<double> {
 };
 
 // multiply by sign*i, sign = -1 (forward) or +1 (inverse)
-template <bool INV, typename T> __device__ __forceinline__ cx<T> mul_si(cx<T> a) {
+template <bool INV, typename T> __host__ __device__ __forceinline__ cx<T> mul_si(cx<T> a) {
     return INV ? cx<T>{-a.y, a.x} : cx<T>{a.y, -a.x};
 }
 
 template <int R, bool INV, typename T> struct Dft;
 
 template <bool INV, typename T> struct Dft<2, INV, T> {
-    __device__ __forceinline__ static void run(cx<T> *v) {
+    static constexpr int out(int p) { return p; }  // natural output order
+    __host__ __device__ __forceinline__ static void run(cx<T> *v) {
         const cx<T> a = v[0], b = v[1];
         v[0] = a + b;
         v[1] = a - b;
     }
 };
 template <bool INV, typename T> struct Dft<4, INV, T> {
-    __device__ __forceinline__ static void run(cx<T> *v) {
+    static constexpr int out(int p) { return p; }  // natural output order
+    __host__ __device__ __forceinline__ static void run(cx<T> *v) {
         const cx<T> t0 = v[0] + v[2], t1 = v[0] - v[2], t2 = v[1] + v[3];
         const cx<T> t3 = mul_si<INV>(v[1] - v[3]);
         v[0] = t0 + t2;
@@ -103,7 +126,8 @@ template <bool INV, typename T> struct Dft<4, INV, T> {
     }
 };
 template <bool INV, typename T> struct Dft<8, INV, T> {
-    __device__ __forceinline__ static void run(cx<T> *v) {
+    static constexpr int out(int p) { return p; }  // natural output order
+    __host__ __device__ __forceinline__ static void run(cx<T> *v) {
         cx<T> e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
         Dft<4, INV, T>::run(e);
         Dft<4, INV, T>::run(o);
@@ -125,7 +149,8 @@ template <bool INV, typename T> struct Dft<8, INV, T> {
     }
 };
 template <bool INV, typename T> struct Dft<3, INV, T> {
-    __device__ __forceinline__ static void run(cx<T> *v) {
+    static constexpr int out(int p) { return p; }  // natural output order
+    __host__ __device__ __forceinline__ static void run(cx<T> *v) {
         const cx<T> a = v[1] + v[2], b = v[1] - v[2];
         const cx<T> A = {v[0].x - T(0.5) * a.x, v[0].y - T(0.5) * a.y};
         const cx<T> iB = mul_si<INV>(cscale(b, DftConst<T>::S3));
@@ -135,7 +160,8 @@ template <bool INV, typename T> struct Dft<3, INV, T> {
     }
 };
 template <bool INV, typename T> struct Dft<5, INV, T> {
-    __device__ __forceinline__ static void run(cx<T> *v) {
+    static constexpr int out(int p) { return p; }  // natural output order
+    __host__ __device__ __forceinline__ static void run(cx<T> *v) {
         using K = DftConst<T>;
         const cx<T> a1 = v[1] + v[4], b1 = v[1] - v[4], a2 = v[2] + v[3], b2 = v[2] - v[3];
         const cx<T> A1 = {v[0].x + a1.x * K::C51 + a2.x * K::C52, v[0].y + a1.y * K::C51 + a2.y * K::C52};
@@ -151,7 +177,8 @@ template <bool INV, typename T> struct Dft<5, INV, T> {
     }
 };
 template <bool INV, typename T> struct Dft<7, INV, T> {
-    __device__ __forceinline__ static void run(cx<T> *v) {
+    static constexpr int out(int p) { return p; }  // natural output order
+    __host__ __device__ __forceinline__ static void run(cx<T> *v) {
         using K = DftConst<T>;
         const cx<T> a1 = v[1] + v[6], b1 = v[1] - v[6];
         const cx<T> a2 = v[2] + v[5], b2 = v[2] - v[5];
@@ -177,10 +204,124 @@ template <bool INV, typename T> struct Dft<7, INV, T> {
     }
 };
 
+// ----------------------------------------------------------------------------- composites
+// Compile-time loop and trigonometry for the composite codelets.
+template <int I, int N, class F> __host__ __device__ __forceinline__ void static_for(F &&f) {
+    if constexpr (I < N) {
+        f(std::integral_constant<int, I>{});
+        static_for<I + 1, N>(f);
+    }
+}
+// cos/sin(2 pi m / R) by Taylor series after reduction to [-pi, pi] (double,
+// evaluated at compile time).
+constexpr double ct_pi = 3.14159265358979323846264338327950288;
+constexpr double ct_series_cos(double x) {
+    double term = 1.0, sum = 1.0;
+    for (int k = 1; k < 24; ++k) {
+        term *= -x * x / ((2.0 * k - 1.0) * (2.0 * k));
+        sum += term;
+    }
+    return sum;
+}
+constexpr double ct_series_sin(double x) {
+    double term = x, sum = x;
+    for (int k = 1; k < 24; ++k) {
+        term *= -x * x / ((2.0 * k) * (2.0 * k + 1.0));
+        sum += term;
+    }
+    return sum;
+}
+constexpr double ct_angle(int m, int R) {
+    const int r = ((m % R) + R) % R;
+    const int c = 2 * r > R ? r - R : r;  // in (-R/2, R/2]
+    return 2.0 * ct_pi * (double)c / (double)R;
+}
+constexpr double ct_cos(int m, int R) { return ct_series_cos(ct_angle(m, R)); }
+constexpr double ct_sin(int m, int R) { return ct_series_sin(ct_angle(m, R)); }
+
+// x * exp(sign * 2 pi i m / R) with m, R compile-time (trivial angles exact).
+template <int M, int R, bool INV, typename T> __host__ __device__ __forceinline__ cx<T> twiddle_ct(cx<T> x) {
+    constexpr int m = ((M % R) + R) % R;
+    if constexpr (m == 0) {
+        return x;
+    } else if constexpr (2 * m == R) {
+        return cx<T>{-x.x, -x.y};
+    } else if constexpr (4 * m == R) {
+        return mul_si<INV>(x);
+    } else if constexpr (4 * m == 3 * R) {
+        return mul_si<!INV>(x);
+    } else {
+        constexpr double c = ct_cos(m, R);
+        constexpr double sn = INV ? ct_sin(m, R) : -ct_sin(m, R);
+        return cx<T>{x.x * (T)c - x.y * (T)sn, x.x * (T)sn + x.y * (T)c};
+    }
+}
+
+template <int R> struct Split;  // R = A * B for the composite radices
+#define UPDC_SPLIT(R_, A_, B_)                      \
+    template <> struct Split<R_> {                  \
+        static constexpr int A = A_, B = B_;        \
+    };
+UPDC_SPLIT(6, 2, 3)
+UPDC_SPLIT(9, 3, 3)
+UPDC_SPLIT(10, 2, 5)
+UPDC_SPLIT(12, 4, 3)
+UPDC_SPLIT(14, 2, 7)
+UPDC_SPLIT(15, 3, 5)
+UPDC_SPLIT(16, 4, 4)
+UPDC_SPLIT(18, 2, 9)
+UPDC_SPLIT(20, 4, 5)
+UPDC_SPLIT(21, 3, 7)
+UPDC_SPLIT(24, 8, 3)
+UPDC_SPLIT(25, 5, 5)
+UPDC_SPLIT(27, 3, 9)
+UPDC_SPLIT(28, 4, 7)
+UPDC_SPLIT(32, 4, 8)
+#undef UPDC_SPLIT
+
+// R = A*B point DFT in place: for each n2 < B the A-point DFT of
+// x[B*n1 + n2] (written back at B*k1 + n2, times w_R^(n2*k1)), then for each
+// k1 the B-point DFT of the B consecutive values v[B*k1 .. B*k1+B).  Register
+// p = B*k1 + q then holds X[k1 + A*out_B(q)]; out() gives that map.
+template <int R, bool INV, typename T> struct DftComposite {
+    static constexpr int A = Split<R>::A, B = Split<R>::B;
+    static constexpr int out(int p) { return p / B + A * Dft<B, INV, T>::out(p % B); }
+    __host__ __device__ __forceinline__ static void run(cx<T> *v) {
+        static_for<0, B>([&](auto n2) {
+            cx<T> a[A];
+            static_for<0, A>([&](auto n1) { a[n1] = v[B * n1 + n2]; });
+            Dft<A, INV, T>::run(a);
+            static_for<0, A>([&](auto q) {
+                constexpr int k1 = Dft<A, INV, T>::out(q);
+                v[B * k1 + n2] = twiddle_ct<(int)n2 * k1, R, INV>(a[q]);
+            });
+        });
+        static_for<0, A>([&](auto k1) { Dft<B, INV, T>::run(v + B * k1); });
+    }
+};
+#define UPDC_COMPOSITE(R_)                                                         \
+    template <bool INV, typename T> struct Dft<R_, INV, T> : DftComposite<R_, INV, T> {};
+UPDC_COMPOSITE(6)
+UPDC_COMPOSITE(9)
+UPDC_COMPOSITE(10)
+UPDC_COMPOSITE(12)
+UPDC_COMPOSITE(14)
+UPDC_COMPOSITE(15)
+UPDC_COMPOSITE(16)
+UPDC_COMPOSITE(18)
+UPDC_COMPOSITE(20)
+UPDC_COMPOSITE(21)
+UPDC_COMPOSITE(24)
+UPDC_COMPOSITE(25)
+UPDC_COMPOSITE(27)
+UPDC_COMPOSITE(28)
+UPDC_COMPOSITE(32)
+#undef UPDC_COMPOSITE
+
 // ----------------------------------------------------------------------------- stages
 template <int R, int K, bool INV, int NT, typename T>
 __device__ __forceinline__ void fft_stage(cx<T> *buf, int n, int batch, int Ns, FastDiv ns_div, FastDiv nb_div,
-                                          const cx<T> *__restrict__ tw) {
+                                          const cx<T> *__restrict__ tw, int sh) {
     const int nb = n / R;
     const int total = nb * batch;
     const int tid = threadIdx.x;
@@ -202,9 +343,9 @@ __device__ __forceinline__ void fft_stage(cx<T> *buf, int n, int batch, int Ns, 
             const int row = batch == 1 ? 0 : (int)nb_div.div((uint32_t)b);
             const int j = b - row * nb;
             const int k = j - (int)ns_div.div((uint32_t)j) * Ns;
-            const cx<T> *base = buf + row * n;
+            const int base = row * n + j;
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[kk][r] = base[j + r * nb];
+            for (int r = 0; r < R; ++r) v[kk][r] = buf[fpad(base + r * nb, sh)];
             if (k) {
                 const cx<T> *t = tw + k * (R - 1);
 #pragma unroll
@@ -222,8 +363,10 @@ __device__ __forceinline__ void fft_stage(cx<T> *buf, int n, int batch, int Ns, 
 #pragma unroll
     for (int kk = 0; kk < K; ++kk) {
         if (ob[kk] >= 0) {
-#pragma unroll
-            for (int r = 0; r < R; ++r) buf[ob[kk] + r * Ns] = v[kk][r];
+            static_for<0, R>([&](auto p) {
+                constexpr int s = Dft<R, INV, T>::out(p);
+                buf[fpad(ob[kk] + s * Ns, sh)] = v[kk][p];
+            });
         }
     }
     __syncthreads();
@@ -252,33 +395,51 @@ __device__ __forceinline__ void load_plan(const FftPlan *__restrict__ g, FftPlan
     __syncthreads();
 }
 
-// Transforms `batch` sequences of length plan.n stored back to back in buf
-// (batch * n <= CAP).  Every thread of the block must call this; `plan` points
-// to the block's shared copy.  Stages are ordered by radix (fft_factor), and
-// each radix gets its own loop so that only one radix's registers are live at
-// a time (a single switch inside one loop makes ptxas spill).
-template <bool INV, int NT, int CAP, typename T>
+// Transforms `batch` sequences of length plan.n stored back to back (logical
+// index b*n + i, shared-memory slot fpad(., plan.pad_shift)) in buf (batch * n <= CAP).
+// Every thread of the block must call this; `plan` points to the block's
+// shared copy, whose radices must not exceed RMAX.  Stages run in descending
+// radix order (fft_factor), one loop per radix, so that only one radix's
+// registers are live at a time (a single switch inside one loop makes ptxas
+// spill).
+template <bool INV, int NT, int CAP, int RMAX, typename T>
 __device__ __forceinline__ void fft_batch(cx<T> *buf, int batch, const FftPlan *plan) {
     // volatile (shared-memory) reads keep the per-stage fields from being
     // hoisted out of the callers' loops (a hoisted copy of the whole plan
     // would spill)
     const volatile FftPlan *vp = plan;
     const cx<T> *tw = reinterpret_cast<const cx<T> *>(vp->tw);
-    const int n = vp->n, nstage = vp->nstage;
+    const int n = vp->n, nstage = vp->nstage, sh = vp->pad_shift;
     int s = 0;
-#define UPDC_FFT_RUN(R)                                                                                   \
-    _Pragma("unroll 1") while (s < nstage && vp->radix[s] == R) {                                                           \
-        fft_stage<R, StageK<R, NT, CAP>::value, INV, NT>(buf, n, batch, vp->ns[s],                       \
-                                                         FastDiv_v(vp->ns_div[s]), FastDiv_v(vp->nb_div[s]), \
-                                                         tw + vp->twoff[s]);                             \
-        ++s;                                                                                             \
+#define UPDC_FFT_RUN(R)                                                                                     \
+    if constexpr (R <= RMAX) {                                                                             \
+        _Pragma("unroll 1") while (s < nstage && vp->radix[s] == R) {                                      \
+            fft_stage<R, StageK<R, NT, CAP>::value, INV, NT>(buf, n, batch, vp->ns[s], FastDiv_v(vp->ns_div[s]), \
+                                                             FastDiv_v(vp->nb_div[s]), tw + vp->twoff[s], sh); \
+            ++s;                                                                                           \
+        }                                                                                                  \
     }
+    UPDC_FFT_RUN(32)
+    UPDC_FFT_RUN(28)
+    UPDC_FFT_RUN(27)
+    UPDC_FFT_RUN(25)
+    UPDC_FFT_RUN(24)
+    UPDC_FFT_RUN(21)
+    UPDC_FFT_RUN(20)
+    UPDC_FFT_RUN(18)
+    UPDC_FFT_RUN(16)
+    UPDC_FFT_RUN(15)
+    UPDC_FFT_RUN(14)
+    UPDC_FFT_RUN(12)
+    UPDC_FFT_RUN(10)
+    UPDC_FFT_RUN(9)
     UPDC_FFT_RUN(8)
-    UPDC_FFT_RUN(4)
-    UPDC_FFT_RUN(2)
     UPDC_FFT_RUN(7)
+    UPDC_FFT_RUN(6)
     UPDC_FFT_RUN(5)
+    UPDC_FFT_RUN(4)
     UPDC_FFT_RUN(3)
+    UPDC_FFT_RUN(2)
 #undef UPDC_FFT_RUN
 }
 

@@ -7,6 +7,7 @@
 
 #include "common.cuh"
 #include "fft.cuh"
+#include "tma.cuh"
 
 namespace updc {
 
@@ -19,10 +20,14 @@ template <int NT, int CAP, typename T> struct MinBlocks {
 };
 
 // ---------------------------------------------------------------------------- loaders
+// Real input of the row transform: value of exposure k, row y, column x.
 template <typename T> struct PlaneLoader {
     const T *p;
     int pitch;
-    __device__ __forceinline__ T operator()(int y, int x) const { return p[(size_t)y * pitch + x]; }
+    size_t batch_stride;
+    __device__ __forceinline__ T operator()(int k, int y, int x) const {
+        return p[k * batch_stride + (size_t)y * pitch + x];
+    }
 };
 
 // Centre-wrapped, normalised PSF on the FW x FH grid (updc_core.c:813-821):
@@ -32,7 +37,7 @@ template <typename T> struct PsfLoader {
     const float *psf;
     int pw, fwid, fhei, FW, FH, transposed;
     T inv;
-    __device__ __forceinline__ T operator()(int yy, int xx) const {
+    __device__ __forceinline__ T operator()(int, int yy, int xx) const {
         const int y = (yy + fhei / 2) % FH, x = (xx + fwid / 2) % FW;
         if (y >= fhei || x >= fwid) return T(0);
         const size_t src = transposed ? (size_t)x * pw + y : (size_t)y * pw + x;
@@ -42,45 +47,90 @@ template <typename T> struct PsfLoader {
     __device__ __forceinline__ static double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 };
 
+// The u-major side of a row transform: either plain loads/stores at
+// spec[k*batch_stride + u*ld + y] (TMA = false) or a 3-D tensor map over the
+// same array (TMA = true, 8-byte elements, box {B*EW, TMA_UBOX, 1}).
+constexpr int TMA_UBOX = 256;
+template <typename T> struct TmaElems {
+    static constexpr int value = sizeof(cx<T>) / 8;  // 8-byte tensor elements per complex value
+};
+struct SpecRef {
+    void *p;
+    int ld;
+    size_t batch_stride;
+};
+
+// Shared layout of a row kernel: the FFT buffer (B*M complex) and, with TMA,
+// a staging tile of nbox*ubox*B complex (ubox = min(256, M+1) u-rows a box).
+// FFT radices are limited to 16 (register budget of 64 per thread).
+constexpr int FFT_RMAX = 16;
+__host__ __device__ inline size_t fft_buf_bytes(int count, size_t csize, int shift) {
+    return ((size_t)fpad_size(count, shift) * csize + 127) / 128 * 128;
+}
+__host__ __device__ inline size_t row_buf_bytes(int B, int M, size_t csize, int shift) { return fft_buf_bytes(B * M, csize, shift); }
+__host__ __device__ inline int row_ubox(int M) { return M + 1 < TMA_UBOX ? M + 1 : TMA_UBOX; }
+__host__ __device__ inline int row_nbox(int M) { return (M + 1 + row_ubox(M) - 1) / row_ubox(M); }
+__host__ __device__ inline size_t row_stage_bytes(int B, int M, size_t csize) {
+    return (size_t)row_nbox(M) * row_ubox(M) * B * csize;
+}
+
 // ---------------------------------------------------------------------------- row R2C
 // Rows [0, rows) of the real plane, zero-padded from W to FW = 2M columns,
 // transformed along x with an M-point complex FFT of z[m] = x[2m] + i x[2m+1]
-// and the split z -> X post-processing; bins are stored u-major.
-template <typename T, int NT, int CAP, class Loader>
-__global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_row_r2c(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ post, Loader ld, int W,
-                                                int rows, int B, cx<T> *__restrict__ out, int ldo, size_t out_batch_stride) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+// and the split z -> X post-processing; bins are stored u-major.  Exposure =
+// blockIdx.y.
+template <typename T, int NT, int CAP, class Loader, bool TMA>
+__global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
+    k_row_r2c(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ post, Loader ld, int W, int rows, int B,
+              SpecRef out, const __grid_constant__ CUtensorMap omap) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
     __shared__ FftPlan s_plan;
     load_plan(plan, &s_plan);
-    const int M = s_plan.n;
+    const int M = s_plan.n, sh = s_plan.pad_shift;
     const int y0 = blockIdx.x * B;
     const int nb = min(B, rows - y0);
-    out += blockIdx.y * out_batch_stride;
-    for (int i = threadIdx.x; i < B * M; i += NT) {
-        const int b = i / M, m = i - b * M;
-        T a = 0, c = 0;
-        if (b < nb) {
-            const int x = 2 * m;
-            if (x < W) a = ld(y0 + b, x);
-            if (x + 1 < W) c = ld(y0 + b, x + 1);
+    const int kexp = blockIdx.y;
+    for (int b = 0; b < B; ++b)
+        for (int m = threadIdx.x; m < M; m += NT) {
+            T a = 0, c = 0;
+            if (b < nb) {
+                const int x = 2 * m;
+                if (x < W) a = ld(kexp, y0 + b, x);
+                if (x + 1 < W) c = ld(kexp, y0 + b, x + 1);
+            }
+            buf[fpad(b * M + m, sh)] = {a, c};
         }
-        buf[i] = {a, c};
-    }
     __syncthreads();
-    fft_batch<false, NT, CAP>(buf, B, &s_plan);
+    fft_batch<false, NT, CAP, FFT_RMAX>(buf, B, &s_plan);
+    cx<T> *stage = reinterpret_cast<cx<T> *>(smem_raw + row_buf_bytes(B, M, sizeof(cx<T>), sh));
+    cx<T> *dst = reinterpret_cast<cx<T> *>(out.p) + kexp * out.batch_stride;
     const T half = T(0.5);
     for (int i = threadIdx.x; i < (M + 1) * B; i += NT) {
         const int u = i / B, b = i - u * B;
-        if (b >= nb) continue;
-        const cx<T> *z = buf + b * M;
-        const cx<T> Z = z[u == M ? 0 : u];
-        const cx<T> Zm = z[u == 0 ? 0 : M - u];
-        const cx<T> Zc = {Zm.x, -Zm.y};
-        const cx<T> E = {half * (Z.x + Zc.x), half * (Z.y + Zc.y)};
-        const cx<T> D = {half * (Z.x - Zc.x), half * (Z.y - Zc.y)};
-        const cx<T> P = fmulc(D, post[u]);
-        out[(size_t)u * ldo + y0 + b] = {E.x + P.y, E.y - P.x};
+        cx<T> X = {0, 0};
+        if (b < nb) {
+            const cx<T> Z = buf[fpad(b * M + (u == M ? 0 : u), sh)];
+            const cx<T> Zm = buf[fpad(b * M + (u == 0 ? 0 : M - u), sh)];
+            const cx<T> Zc = {Zm.x, -Zm.y};
+            const cx<T> E = {half * (Z.x + Zc.x), half * (Z.y + Zc.y)};
+            const cx<T> D = {half * (Z.x - Zc.x), half * (Z.y - Zc.y)};
+            const cx<T> P = fmulc(D, post[u]);
+            X = {E.x + P.y, E.y - P.x};
+        }
+        if (TMA) stage[i] = X;
+        else if (b < nb) dst[(size_t)u * out.ld + y0 + b] = X;
+    }
+    if (TMA) {
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            constexpr int EW = TmaElems<T>::value;
+            const int ub = row_ubox(M);
+            for (int bx = 0; bx < row_nbox(M); ++bx)
+                tma_store_3d(&omap, stage + (size_t)bx * ub * B, y0 * EW, bx * ub, kexp);
+            tma_store_commit_and_wait();
+        }
     }
 }
 
@@ -97,25 +147,51 @@ template <typename T> struct PlaneStore {
 // Inverse of k_row_r2c for rows [0, rows): bins u-major in `in`, output
 // x in [0, W) of each row times `scale` (the crop of updc_core.c:765-766).
 // The imaginary parts of the DC and Nyquist bins are ignored, as FFTW does.
-template <typename T, int NT, int CAP, class Epi>
-__global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_row_c2r(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ post, const cx<T> *__restrict__ in,
-                                                int ldi, size_t in_batch_stride, int rows, int W, int B, T scale, Epi epi) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+// With TMA the block's {B rows} x {all u} tile arrives through the tensor map.
+template <typename T, int NT, int CAP, class Epi, bool TMA>
+__global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
+    k_row_c2r(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ post, SpecRef in,
+              const __grid_constant__ CUtensorMap imap, int rows, int W, int B, T scale, Epi epi,
+              unsigned long long *__restrict__ err) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
     __shared__ FftPlan s_plan;
+    __shared__ __align__(8) uint64_t bar;
     load_plan(plan, &s_plan);
-    const int M = s_plan.n;
+    const int M = s_plan.n, sh = s_plan.pad_shift;
     const int y0 = blockIdx.x * B;
     const int nb = min(B, rows - y0);
     const int kexp = blockIdx.y;
-    in += kexp * in_batch_stride;
+    cx<T> *stage = reinterpret_cast<cx<T> *>(smem_raw + row_buf_bytes(B, M, sizeof(cx<T>), sh));
+    const cx<T> *src = reinterpret_cast<const cx<T> *>(in.p) + kexp * in.batch_stride;
+    if (TMA) {
+        if (threadIdx.x == 0) mbar_init(&bar, 1);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            constexpr int EW = TmaElems<T>::value;
+            const int nbox = row_nbox(M), ub = row_ubox(M);
+            mbar_arrive_expect_tx(&bar, (uint32_t)row_stage_bytes(B, M, sizeof(cx<T>)));
+            for (int bx = 0; bx < nbox; ++bx)
+                tma_load_3d(stage + (size_t)bx * ub * B, &imap, &bar, y0 * EW, bx * ub, kexp);
+        }
+        if (!mbar_wait_bounded(&bar, 0)) {
+            if (threadIdx.x == 0)
+                atomicMin(err, (unsigned long long)make_error_key(STAGE_UPDATE, blockIdx.x, ERR_DEVICE_TIMEOUT));
+            return;
+        }
+    }
     for (int i = threadIdx.x; i < M * B; i += NT) {
         const int k = i / B, b = i - k * B;
         cx<T> Zp = {0, 0};
         if (b < nb) {
-            const int y = y0 + b;
-            cx<T> X = in[(size_t)k * ldi + y];
-            cx<T> Xm = in[(size_t)(M - k) * ldi + y];
+            cx<T> X, Xm;
+            if (TMA) {
+                X = stage[i];
+                Xm = stage[(M - k) * B + b];
+            } else {
+                X = src[(size_t)k * in.ld + y0 + b];
+                Xm = src[(size_t)(M - k) * in.ld + y0 + b];
+            }
             if (k == 0) { X.y = 0; Xm.y = 0; }
             const cx<T> S = {X.x + Xm.x, X.y - Xm.y};
             const cx<T> D = {X.x - Xm.x, X.y + Xm.y};
@@ -123,15 +199,15 @@ __global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_row_c2r(
             const cx<T> Q = fmulc_conj(D, w);
             Zp = {S.x - Q.y, S.y + Q.x};
         }
-        buf[b * M + k] = Zp;
+        buf[fpad(b * M + k, sh)] = Zp;
     }
     __syncthreads();
-    fft_batch<true, NT, CAP>(buf, B, &s_plan);
-    for (int i = threadIdx.x; i < nb * W; i += NT) {
-        const int b = i / W, x = i - b * W;
-        const cx<T> z = buf[b * M + (x >> 1)];
-        epi(kexp, y0 + b, x, mul_scale((x & 1) ? z.y : z.x, scale));
-    }
+    fft_batch<true, NT, CAP, FFT_RMAX>(buf, B, &s_plan);
+    for (int b = 0; b < nb; ++b)
+        for (int x = threadIdx.x; x < W; x += NT) {
+            const cx<T> z = buf[fpad(b * M + (x >> 1), sh)];
+            epi(kexp, y0 + b, x, mul_scale((x & 1) ? z.y : z.x, scale));
+        }
 }
 
 
@@ -152,28 +228,31 @@ __global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_forw
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
     __shared__ FftPlan s_plan;
     load_plan(plan, &s_plan);
-    const int n = s_plan.n;
+    const int n = s_plan.n, sh = s_plan.pad_shift;
     const int u = blockIdx.x;
-    cx<T> *xh = aux ? aux + (size_t)u * n : buf + ((n * sizeof(cx<T>) + 15) / 16) * (16 / sizeof(cx<T>));
+    cx<T> *xh = aux ? aux + (size_t)u * n : reinterpret_cast<cx<T> *>(smem_raw + fft_buf_bytes(n, sizeof(cx<T>), sh));
     const cx<T> *src = rx + (size_t)u * ldr;
 #pragma unroll 1
     for (int it = 0; it <= nexp; ++it) {
         if (it == 0) {
-            for (int v = threadIdx.x; v < n; v += NT) buf[v] = v < rows_in ? src[v] : cx<T>{0, 0};
+            for (int v = threadIdx.x; v < n; v += NT) buf[fpad(v, sh)] = v < rows_in ? src[v] : cx<T>{0, 0};
         } else {
             const cx<T> *kr = khat + (it - 1) * khat_stride + (size_t)u * n;
             for (int v = threadIdx.x; v < n; v += NT) {
                 const cx<T> p = cmul(xh[v], kr[v]);
-                buf[v] = {p.x, -p.y};
+                buf[fpad(v, sh)] = {p.x, -p.y};
             }
         }
         __syncthreads();
-        fft_batch<false, NT, CAP>(buf, 1, &s_plan);
+        fft_batch<false, NT, CAP, FFT_RMAX>(buf, 1, &s_plan);
         if (it == 0) {
-            for (int v = threadIdx.x; v < n; v += NT) xh[v] = buf[v];
+            for (int v = threadIdx.x; v < n; v += NT) xh[v] = buf[fpad(v, sh)];
         } else {
             cx<T> *dst = y + (it - 1) * y_stride + (size_t)u * ldy;
-            for (int v = threadIdx.x; v < rows_out; v += NT) dst[v] = {buf[v].x, -buf[v].y};
+            for (int v = threadIdx.x; v < rows_out; v += NT) {
+                const cx<T> q = buf[fpad(v, sh)];
+                dst[v] = {q.x, -q.y};
+            }
         }
         __syncthreads();
     }
@@ -233,30 +312,33 @@ __global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_adjo
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
     __shared__ FftPlan s_plan;
     load_plan(plan, &s_plan);
-    const int n = s_plan.n;
+    const int n = s_plan.n, sh = s_plan.pad_shift;
     const int u = blockIdx.x;
     typename Acc::S *acc = aux ? aux + (size_t)u * n
-                               : reinterpret_cast<typename Acc::S *>(smem_raw + ((n * sizeof(cx<T>) + 15) / 16) * 16);
+                               : reinterpret_cast<typename Acc::S *>(smem_raw + fft_buf_bytes(n, sizeof(cx<T>), sh));
     for (int v = threadIdx.x; v < n; v += NT) Acc::zero(acc[v]);
 #pragma unroll 1
     for (int it = 0; it <= nexp; ++it) {
         if (it < nexp) {
             const cx<T> *src = rs + it * rs_stride + (size_t)u * ldr;
-            for (int v = threadIdx.x; v < n; v += NT) buf[v] = v < rows_in ? src[v] : cx<T>{0, 0};
+            for (int v = threadIdx.x; v < n; v += NT) buf[fpad(v, sh)] = v < rows_in ? src[v] : cx<T>{0, 0};
         } else {
             for (int v = threadIdx.x; v < n; v += NT) {
                 const cx<T> a = Acc::get(acc[v]);
-                buf[v] = {a.x, -a.y};
+                buf[fpad(v, sh)] = {a.x, -a.y};
             }
         }
         __syncthreads();
-        fft_batch<false, NT, CAP>(buf, 1, &s_plan);
+        fft_batch<false, NT, CAP, FFT_RMAX>(buf, 1, &s_plan);
         if (it < nexp) {
             const cx<T> *kr = khat + it * khat_stride + (size_t)u * n;
-            for (int v = threadIdx.x; v < n; v += NT) Acc::add(acc[v], buf[v], kr[v]);
+            for (int v = threadIdx.x; v < n; v += NT) Acc::add(acc[v], buf[fpad(v, sh)], kr[v]);
         } else {
             cx<T> *dst = c + (size_t)u * ldc;
-            for (int v = threadIdx.x; v < rows_out; v += NT) dst[v] = {buf[v].x, -buf[v].y};
+            for (int v = threadIdx.x; v < rows_out; v += NT) {
+                const cx<T> q = buf[fpad(v, sh)];
+                dst[v] = {q.x, -q.y};
+            }
         }
         __syncthreads();
     }
@@ -270,14 +352,14 @@ __global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_fft(
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
     __shared__ FftPlan s_plan;
     load_plan(plan, &s_plan);
-    const int n = s_plan.n;
+    const int n = s_plan.n, sh = s_plan.pad_shift;
     const int u = blockIdx.x;
     const cx<T> *src = in + (size_t)u * ldi;
-    for (int v = threadIdx.x; v < n; v += NT) buf[v] = v < rows_in ? src[v] : cx<T>{0, 0};
+    for (int v = threadIdx.x; v < n; v += NT) buf[fpad(v, sh)] = v < rows_in ? src[v] : cx<T>{0, 0};
     __syncthreads();
-    fft_batch<INV, NT, CAP>(buf, 1, &s_plan);
+    fft_batch<INV, NT, CAP, FFT_RMAX>(buf, 1, &s_plan);
     cx<T> *dst = out + (size_t)u * ldo;
-    for (int v = threadIdx.x; v < rows_out; v += NT) dst[v] = buf[v];
+    for (int v = threadIdx.x; v < rows_out; v += NT) dst[v] = buf[fpad(v, sh)];
 }
 
 }  // namespace updc

@@ -63,27 +63,17 @@ constexpr int DET_WARPS = 8;
 constexpr int DET_LCAP = 384;
 
 template <typename T> struct LinkSum {
-    T s = T(0), c = T(0);
+    // COMP: the sum runs in FP64 (products of FP32 operands are exact in
+    // FP64), and raw_mu is that sum plus the offset rounded once to T.
+    T s = T(0);
+    double d = 0.0;
     template <bool COMP> __device__ __forceinline__ void add(float f, T bl) {
-        if (!COMP) {
-            s = fma_rn((T)f, bl, s);
-        } else {  // Dot2: error-free product and sum
-            const T a = (T)f;
-            const T h = mul_rn(a, bl);
-            const T r = fma_rn(a, bl, -h);
-            const T s2 = add_rn(s, h);
-            const T bb = sub_rn(s2, s);
-            const T q = add_rn(sub_rn(s, sub_rn(s2, bb)), sub_rn(h, bb));
-            s = s2;
-            c = add_rn(c, add_rn(q, r));
-        }
+        if (!COMP) s = fma_rn((T)f, bl, s);
+        else d = __fma_rn((double)f, (double)bl, d);
     }
     template <bool COMP> __device__ __forceinline__ T finish(T offset) const {
         if (!COMP) return add_rn(s, offset);
-        const T s2 = add_rn(s, offset);
-        const T bb = sub_rn(s2, s);
-        const T q = add_rn(sub_rn(s, sub_rn(s2, bb)), sub_rn(offset, bb));
-        return add_rn(s2, add_rn(c, q));
+        return (T)__dadd_rn(d, (double)offset);
     }
 };
 
@@ -91,9 +81,9 @@ template <typename T> struct LinkSum {
 //   pred = sum_z fmaf(frac[z], blur[t(z)], pred) in link order;
 //   raw_mu = pred + (background + pedestal);  FreezeMu;  ratio;  wr = W * ratio.
 // Writes wr (0 for skipped pixels) for the adjoint gather.  With COMP the
-// prediction is an error-free-transformation dot product (Ogita-Rump-Oishi
-// Dot2) and raw_mu its correctly rounded sum with the offset, so the
-// FreezeMu threshold is decided on a compensated raw_mu.
+// prediction is accumulated in FP64 and raw_mu is rounded once from the FP64
+// sum with the offset, so the FreezeMu threshold is decided on a compensated
+// raw_mu.
 template <typename T, bool COMP>
 __global__ void __launch_bounds__(DET_WARPS * 32) k_detector(const ExpDesc<T> *__restrict__ exps, size_t nin, size_t nout,
                                                            const T *__restrict__ blur_all, T *__restrict__ wr_all,
@@ -110,28 +100,58 @@ __global__ void __launch_bounds__(DET_WARPS * 32) k_detector(const ExpDesc<T> *_
     for (size_t p0 = ((size_t)blockIdx.x * DET_WARPS + warp) * 32; p0 < nin; p0 += step) {
         const size_t p = p0 + lane;
         const bool valid = p < nin;
+        // every per-pixel load first (independent of each other)
         const uint32_t z0 = valid ? e.off[p] : 0u, z1 = valid ? e.off[p + 1] : 0u;
+        const T w = valid ? e.wht[p] : T(0);
+        const uint32_t bse = (valid && e.delta16) ? e.base[p] : 0u;
+        const T sci = valid ? e.sci[p] : T(0);
+        uint8_t fz = valid ? e.frozen[p] : (uint8_t)0;
         const int last = (int)min((size_t)31, nin - 1 - p0);
         const uint32_t zb = __shfl_sync(0xffffffffu, z0, 0);
         const uint32_t ze = __shfl_sync(0xffffffffu, z1, last);
-        const bool staged = ze - zb <= (uint32_t)DET_LCAP;
+        const uint32_t cnt = ze - zb;
+        const bool staged = cnt <= (uint32_t)DET_LCAP;
         if (staged) {
-            for (uint32_t i = lane; i < ze - zb; i += 32) {
-                s_frac[warp][i] = e.frac[zb + i];
-                s_idx[warp][i] = e.delta16 ? (uint32_t)e.delta[zb + i] : e.tgt[zb + i];
+            // all staging loads are issued before any store
+            constexpr int NS = DET_LCAP / 32;
+            float fv[NS];
+            uint32_t iv[NS];
+#pragma unroll
+            for (int j = 0; j < NS; ++j) {
+                const uint32_t i = lane + 32u * j;
+                fv[j] = i < cnt ? e.frac[zb + i] : 0.0f;
+                iv[j] = i < cnt ? (e.delta16 ? (uint32_t)e.delta[zb + i] : e.tgt[zb + i]) : 0u;
+            }
+#pragma unroll
+            for (int j = 0; j < NS; ++j) {
+                const uint32_t i = lane + 32u * j;
+                if (i < cnt) {
+                    s_frac[warp][i] = fv[j];
+                    s_idx[warp][i] = iv[j];
+                }
             }
         }
         __syncwarp();
         T out = T(0);
         if (valid) {
-            const T w = e.wht[p];
             if (w > T(0) && z0 != z1) {
-                const uint32_t bse = e.delta16 ? e.base[p] : 0u;
                 LinkSum<T> acc;
                 if (staged) {
-                    for (uint32_t z = z0; z < z1; ++z) {
-                        const uint32_t j = z - zb;
-                        acc.template add<COMP>(s_frac[warp][j], blur[bse + s_idx[warp][j]]);
+                    // gathers of a chunk are issued together, then the ordered sum
+                    constexpr int CH = 4;
+                    for (uint32_t zc = z0; zc < z1; zc += CH) {
+                        T bl[CH];
+                        float fr[CH];
+#pragma unroll
+                        for (int i = 0; i < CH; ++i) {
+                            const bool ok = zc + i < z1;
+                            const uint32_t j = ok ? zc + i - zb : 0u;
+                            fr[i] = s_frac[warp][j];
+                            bl[i] = ok ? blur[bse + s_idx[warp][j]] : T(0);
+                        }
+#pragma unroll
+                        for (int i = 0; i < CH; ++i)
+                            if (zc + i < z1) acc.template add<COMP>(fr[i], bl[i]);
                     }
                 } else {
                     for (uint32_t z = z0; z < z1; ++z) {
@@ -145,7 +165,6 @@ __global__ void __launch_bounds__(DET_WARPS * 32) k_detector(const ExpDesc<T> *_
                 } else {
                     const unsigned long long o = double_to_ordered((double)raw_mu);
                     mn = o < mn ? o : mn;
-                    uint8_t fz = e.frozen[p];
                     if (!fz && !(raw_mu > T(0))) {
                         fz = 1;
                         e.frozen[p] = 1;
@@ -156,7 +175,7 @@ __global__ void __launch_bounds__(DET_WARPS * 32) k_detector(const ExpDesc<T> *_
                         ++ntot;
                         ratio = T(1);
                     } else {
-                        const T y = add_rn(e.sci[p], e.pedestal);
+                        const T y = add_rn(sci, e.pedestal);
                         ratio = div_rn(y, raw_mu);
                         if (!isfinite(ratio)) record_error(err, STAGE_DETECTOR, (uint64_t)k * nin + p, ERR_NONFINITE_RATIO);
                     }
@@ -194,56 +213,47 @@ __global__ void __launch_bounds__(DET_WARPS * 32) k_detector(const ExpDesc<T> *_
 // ---------------------------------------------------------------------------- adjoint gather
 // scatter_k[t] = sum over the transposed entries of t, in increasing source
 // pixel order, of fmaf(frac, value[p], acc): the exact sequence of
-// updc_core.c:1173-1176 for target t.  ACC may be wider than T.  Entries of a
-// warp's 32 consecutive targets are one contiguous range, staged in shared
-// memory with coalesced loads as in k_detector.
-constexpr int GATHER_LCAP = 256;
-
+// updc_core.c:1173-1176 for target t.  ACC may be wider than T.  Entries are
+// read in chunks: all loads of a chunk first, then the ordered fma chain.
 template <typename T, typename ACC, typename V>
-__global__ void __launch_bounds__(DET_WARPS * 32) k_scatter_t(const ExpDesc<T> *__restrict__ exps, size_t nin, size_t nout,
-                                                            const V *__restrict__ val_all, int use_weight,
-                                                            ACC *__restrict__ out_all) {
-    __shared__ uint32_t s_src[DET_WARPS][GATHER_LCAP];
-    __shared__ float s_frac[DET_WARPS][GATHER_LCAP];
+__global__ void __launch_bounds__(256) k_scatter_t(const ExpDesc<T> *__restrict__ exps, size_t nin, size_t nout,
+                                                   const V *__restrict__ val_all, int use_weight, ACC *__restrict__ out_all) {
     const int k = blockIdx.y;
     const ExpDesc<T> e = exps[k];
     const V *val = use_weight ? nullptr : val_all + k * nin;
     ACC *out = out_all + k * nout;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const size_t step = (size_t)gridDim.x * DET_WARPS * 32;
-    for (size_t t0 = ((size_t)blockIdx.x * DET_WARPS + warp) * 32; t0 < nout; t0 += step) {
-        const size_t t = t0 + lane;
-        const bool valid = t < nout;
-        const uint32_t a = valid ? e.toff[t] : 0u, b = valid ? e.toff[t + 1] : 0u;
-        const int last = (int)min((size_t)31, nout - 1 - t0);
-        const uint32_t eb = __shfl_sync(0xffffffffu, a, 0);
-        const uint32_t ee = __shfl_sync(0xffffffffu, b, last);
-        const bool staged = ee - eb <= (uint32_t)GATHER_LCAP;
-        if (staged) {
-            for (uint32_t i = lane; i < ee - eb; i += 32) {
-                s_src[warp][i] = e.tsrc[eb + i];
-                s_frac[warp][i] = e.tfrac[eb + i];
+    constexpr int CH = 4;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nout; t += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t a = e.toff[t], b = e.toff[t + 1];
+        ACC acc = ACC(0);
+        for (uint32_t ic = a; ic < b; ic += CH) {
+            uint32_t src[CH];
+            float fr[CH];
+            ACC v[CH];
+            bool use[CH];
+#pragma unroll
+            for (int i = 0; i < CH; ++i) {
+                const bool ok = ic + i < b;
+                src[i] = ok ? e.tsrc[ic + i] : 0u;
+                fr[i] = ok ? e.tfrac[ic + i] : 0.0f;
             }
-        }
-        __syncwarp();
-        if (valid) {
-            ACC acc = ACC(0);
-            for (uint32_t i = a; i < b; ++i) {
-                const uint32_t src = staged ? s_src[warp][i - eb] : e.tsrc[i];
-                const float fr = staged ? s_frac[warp][i - eb] : e.tfrac[i];
-                ACC v;
+#pragma unroll
+            for (int i = 0; i < CH; ++i) {
+                const bool ok = ic + i < b;
                 if (use_weight) {
-                    const T w = e.wht[src];
-                    if (!(w > T(0))) continue;  // masked pixels are skipped (updc_core.c:1061)
-                    v = (ACC)w;
+                    const T w = ok ? e.wht[src[i]] : T(0);
+                    use[i] = ok && w > T(0);  // masked pixels are skipped (updc_core.c:1061)
+                    v[i] = (ACC)w;
                 } else {
-                    v = (ACC)val[src];
+                    use[i] = ok;
+                    v[i] = ok ? (ACC)val[src[i]] : ACC(0);
                 }
-                acc = fma_rn((ACC)fr, v, acc);
             }
-            out[t] = acc;
+#pragma unroll
+            for (int i = 0; i < CH; ++i)
+                if (use[i]) acc = fma_rn((ACC)fr[i], v[i], acc);
         }
-        __syncwarp();
+        out[t] = acc;
     }
 }
 
