@@ -230,6 +230,34 @@ def cpu_baseline_sample(ds, w):
                       f"(fft_workers={fftw}, exposure_workers={w.nexp}, FFTW-API shim FFT)"}
 
 
+def fp64_comparison(eng, ds, w, args, device):
+    """The metric's accuracy side: run the FP64 form (the GPU oracle) on the
+    same inputs to the workload's full iteration count, bring the timed engine
+    to the same count, and report the relative RMS of x, the FreezeMu masks
+    that differ, and the FP64 form's own device ms/iteration."""
+    import numpy as np
+    from updc_b200.engine import Engine
+    done = eng.iterations_done
+    target = max(w.iterations, done)
+    if target > done:
+        eng.iterate(target - done, check_each=False)
+    ref = Engine(form="fp64", device=device)
+    ref.load(str(ds.manifest), w.W, w.H, w.iw, w.ih, w.nexp).setup()
+    warm = 3
+    st = ref.iterate(target, check_each=False)
+    ms64 = 1000.0 * sum(s.seconds for s in st[warm:]) / max(1, target - warm)
+    x32 = eng.plane("estimate", as_double=True)
+    x64 = ref.plane("estimate", as_double=True)
+    d = x32 - x64
+    rel_rms = float(np.sqrt(np.mean(d * d) / np.mean(x64 * x64)))
+    mask = np.abs(x64) > 1e-8 * np.abs(x64).max()
+    max_rel = float(np.max(np.abs(d[mask]) / np.abs(x64[mask])))
+    mism = sum(int(np.count_nonzero(eng.plane("frozen", k) != ref.plane("frozen", k))) for k in range(w.nexp))
+    ref.close()
+    return {"iterations": target, "rel_rms": rel_rms, "max_rel_masked": max_rel, "frozen_mismatch": mism,
+            "fp64_ms_per_iteration": round(ms64, 4)}
+
+
 def b200_arm(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -292,6 +320,9 @@ def b200_arm(args, rank, world, local_rank):
         eng.read_plane_into("estimate", x)
     e2e_ms = 1000.0 * (time.time() - t0) / e2e_steps
     nout = w.W * w.H
+    fp64 = None
+    if args.form != "fp64" and not args.no_fp64_check:
+        fp64 = fp64_comparison(eng, ds, w, args, local_rank)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(ds, w)
@@ -315,6 +346,8 @@ def b200_arm(args, rank, world, local_rank):
         "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": x.itemsize * nout,
                 "d2h_bytes_per_step": x.itemsize * nout},
         "cufft_reference": cufft,
+        "fp64_check": fp64,
+        "speedup_vs_fp64": round(fp64["fp64_ms_per_iteration"] / ms, 3) if fp64 else None,
         "gpu_launches": launches_per_iter * args.steps,
         "clocks": clocks.summary(),
     }
@@ -339,6 +372,8 @@ def main():
     p.add_argument("--form", default="fp32", choices=["fp32", "fp64", "fp32-kahan", "fp32-reference"])
     p.add_argument("--data-dir", default=None)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-fp64-check", action="store_true",
+                   help="skip the FP64-form run that gives the metric's accuracy side")
     args = p.parse_args()
     rank, world, local_rank = env_rank()
     if args.impl == "reference":

@@ -28,7 +28,8 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-r
 # geometry must not contract multiply-adds (bit-exact LinkMaps)
 PER_FILE = {"linkmap.cu": ["-fmad=false"]}
 SOURCES = ["linkmap.cu", "engine.cu", "capi.cu"]
-HEADERS = ["common.cuh", "fft.cuh", "kernels.cuh", "pointwise.cuh", "engine.cuh", "geometry.cuh", "linkmap.cuh"]
+HEADERS = ["common.cuh", "fft.cuh", "kernels.cuh", "pointwise.cuh", "engine.cuh", "geometry.cuh", "linkmap.cuh",
+           "tma.cuh"]
 
 
 def nvcc() -> str:

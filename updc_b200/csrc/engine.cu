@@ -513,7 +513,6 @@ template <typename T> class EngineImpl final : public Engine {
     float stage_ms_[8] = {};
 
     FftPlan plan_m_, plan_h_;
-    const FftPlan *d_plan_m_ = nullptr, *d_plan_h_ = nullptr;
     cx<T> *post_ = nullptr;
     T *estimate_ = nullptr, *coverage_ = nullptr, *den_ = nullptr, *correction_ = nullptr;
     T *blur_ = nullptr, *wr_ = nullptr, *scatter_ = nullptr, *sci_ = nullptr, *wht_ = nullptr;
@@ -547,12 +546,6 @@ template <typename T> class EngineImpl final : public Engine {
         pinned_bytes_ = bytes;
     }
 
-    const FftPlan *upload_plan(const FftPlan &p) {
-        FftPlan *d = alloc<FftPlan>(1);
-        UPDC_CUDA(cudaMemcpy(d, &p, sizeof(FftPlan), cudaMemcpyHostToDevice));
-        return d;
-    }
-
     bool acc_fp64() const { return opt_.form == FORM_FP32 && sizeof(T) == 4; }
 
     void choose_fft_shape() {
@@ -579,8 +572,6 @@ template <typename T> class EngineImpl final : public Engine {
         UPDC_CUDA(cudaMemcpy(dh, th.data(), th.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
         plan_m_.tw = dm;
         plan_h_.tw = dh;
-        d_plan_m_ = upload_plan(plan_m_);
-        d_plan_h_ = upload_plan(plan_h_);
         std::vector<cx<T>> post(M_ + 1);
         const double two_pi = 6.283185307179586476925286766559;
         for (int u = 0; u <= M_; ++u) post[u] = cx<T>{(T)std::cos(-two_pi * u / FW_), (T)std::sin(-two_pi * u / FW_)};
@@ -698,19 +689,19 @@ template <typename T> class EngineImpl final : public Engine {
         const SpecRef ref{out, ldh_, (size_t)(M_ + 1) * ldh_};
         if (use_tma_)
             k_row_r2c<T, NT, Caps<T>::ROW, PlaneLoader<T>, true><<<grid, NT, row_smem(), stream_>>>(
-                d_plan_m_, post_, ld, W_, H_, B, ref, map);
+                plan_m_, post_, ld, W_, H_, B, FastDiv((uint32_t)B), ref, map);
         else
             k_row_r2c<T, NT, Caps<T>::ROW, PlaneLoader<T>, false><<<grid, NT, row_smem(), stream_>>>(
-                d_plan_m_, post_, ld, W_, H_, B, ref, no_map_);
+                plan_m_, post_, ld, W_, H_, B, FastDiv((uint32_t)B), ref, no_map_);
         UPDC_CUDA(cudaGetLastError());
     }
     void launch_col_forward() {
         const size_t nu = (size_t)M_ + 1;
         const size_t ks = nu * FH_, ys = nu * ldh_;
         if (FH_ <= Caps<T>::COL_S)
-            k_col_forward<T, NT, Caps<T>::COL_S><<<(unsigned)nu, NT, fwd_smem(), stream_>>>(d_plan_h_, rx_, ldh_, H_, khat_, ks, nexp_, y_, ldh_, ys, H_, (int)nu, aux_fwd_);
+            k_col_forward<T, NT, Caps<T>::COL_S><<<(unsigned)nu, NT, fwd_smem(), stream_>>>(plan_h_, rx_, ldh_, H_, khat_, ks, nexp_, y_, ldh_, ys, H_, (int)nu, aux_fwd_);
         else
-            k_col_forward<T, NT, Caps<T>::COL_L><<<(unsigned)nu, NT, fwd_smem(), stream_>>>(d_plan_h_, rx_, ldh_, H_, khat_, ks, nexp_, y_, ldh_, ys, H_, (int)nu, aux_fwd_);
+            k_col_forward<T, NT, Caps<T>::COL_L><<<(unsigned)nu, NT, fwd_smem(), stream_>>>(plan_h_, rx_, ldh_, H_, khat_, ks, nexp_, y_, ldh_, ys, H_, (int)nu, aux_fwd_);
         UPDC_CUDA(cudaGetLastError());
     }
     template <class Acc> void launch_col_adjoint_t(const cx<T> *khat) {
@@ -722,9 +713,9 @@ template <typename T> class EngineImpl final : public Engine {
         }
         const size_t s = adj_smem<Acc>();
         if (FH_ <= Caps<T>::COL_S)
-            k_col_adjoint<T, Acc, NtAdj<T>::value, Caps<T>::COL_S><<<(unsigned)nu, NtAdj<T>::value, s, stream_>>>(d_plan_h_, rs_, ldh_, nu * ldh_, H_, khat, nu * FH_, nexp_, cr_, ldh_, H_, aux);
+            k_col_adjoint<T, Acc, NtAdj<T>::value, Caps<T>::COL_S><<<(unsigned)nu, NtAdj<T>::value, s, stream_>>>(plan_h_, rs_, ldh_, nu * ldh_, H_, khat, nu * FH_, nexp_, cr_, ldh_, H_, aux);
         else
-            k_col_adjoint<T, Acc, NtAdj<T>::value, Caps<T>::COL_L><<<(unsigned)nu, NtAdj<T>::value, s, stream_>>>(d_plan_h_, rs_, ldh_, nu * ldh_, H_, khat, nu * FH_, nexp_, cr_, ldh_, H_, aux);
+            k_col_adjoint<T, Acc, NtAdj<T>::value, Caps<T>::COL_L><<<(unsigned)nu, NtAdj<T>::value, s, stream_>>>(plan_h_, rs_, ldh_, nu * ldh_, H_, khat, nu * FH_, nexp_, cr_, ldh_, H_, aux);
         UPDC_CUDA(cudaGetLastError());
     }
     void launch_col_adjoint() {
@@ -741,10 +732,10 @@ template <typename T> class EngineImpl final : public Engine {
         const SpecRef ref{const_cast<cx<T> *>(in), ldh_, (size_t)(M_ + 1) * ldh_};
         if (use_tma_)
             k_row_c2r<T, NT, Caps<T>::ROW, PlaneStore<T>, true><<<grid, NT, row_smem(), stream_>>>(
-                d_plan_m_, post_, ref, map, H_, W_, B, scale, PlaneStore<T>{out, W_, nout_}, d_err_);
+                plan_m_, post_, ref, map, H_, W_, B, FastDiv((uint32_t)B), scale, PlaneStore<T>{out, W_, nout_}, d_err_);
         else
             k_row_c2r<T, NT, Caps<T>::ROW, PlaneStore<T>, false><<<grid, NT, row_smem(), stream_>>>(
-                d_plan_m_, post_, ref, no_map_, H_, W_, B, scale, PlaneStore<T>{out, W_, nout_}, d_err_);
+                plan_m_, post_, ref, no_map_, H_, W_, B, FastDiv((uint32_t)B), scale, PlaneStore<T>{out, W_, nout_}, d_err_);
         UPDC_CUDA(cudaGetLastError());
     }
     T scale_factor() const {
@@ -963,7 +954,7 @@ template <typename T> class EngineImpl final : public Engine {
 
     // PSF spectra K_k (u-major, (M+1) x FH) of precision U into dst.
     template <typename U>
-    void psf_spectra(cx<U> *dst, bool fp64_sum, const FftPlan *pm, const FftPlan *ph, const FftPlan &hpm, const FftPlan &hph,
+    void psf_spectra(cx<U> *dst, bool fp64_sum, const FftPlan &pm, const FftPlan &ph,
                      const cx<U> *post) {
         const size_t nu = (size_t)M_ + 1;
         cx<U> *rp = dalloc<cx<U>>(nu * FH_, nullptr);
@@ -1002,12 +993,12 @@ template <typename T> class EngineImpl final : public Engine {
             PsfLoader<U> ld{dp, e.psf_width, transposed_ ? e.psf_height : e.psf_width,
                             transposed_ ? e.psf_width : e.psf_height, FW_, FH_, transposed_, inv};
             const int B = Caps<U>::ROW / M_;
-            const size_t rsm = row_buf_bytes(B, M_, sizeof(cx<U>), hpm.pad_shift);
+            const size_t rsm = row_buf_bytes(B, M_, sizeof(cx<U>), pm.pad_shift);
             set_smem(k_row_r2c<U, NT, Caps<U>::ROW, PsfLoader<U>, false>, rsm);
             dim3 grid((unsigned)ceil_div(FH_, B), 1);
             k_row_r2c<U, NT, Caps<U>::ROW, PsfLoader<U>, false><<<grid, NT, rsm, stream_>>>(
-                pm, post, ld, FW_, FH_, B, SpecRef{rp, FH_, 0}, no_map_);
-            const size_t cs = fft_buf_bytes(FH_, sizeof(cx<U>), hph.pad_shift);
+                pm, post, ld, FW_, FH_, B, FastDiv((uint32_t)B), SpecRef{rp, FH_, 0}, no_map_);
+            const size_t cs = fft_buf_bytes(FH_, sizeof(cx<U>), ph.pad_shift);
             cx<U> *out = dst + (size_t)k * nu * FH_;
             if (FH_ <= Caps<U>::COL_S) {
                 set_smem(k_col_fft<U, NT, Caps<U>::COL_S, false>, cs);
@@ -1025,7 +1016,7 @@ template <typename T> class EngineImpl final : public Engine {
 
     void prepare_psf_spectra() {
         const bool fp64_sum = opt_.form == FORM_FP32 || opt_.form == FORM_FP64;
-        psf_spectra<T>(khat_, fp64_sum, d_plan_m_, d_plan_h_, plan_m_, plan_h_, post_);
+        psf_spectra<T>(khat_, fp64_sum, plan_m_, plan_h_, post_);
     }
 
     void drizzle() {
@@ -1063,16 +1054,13 @@ template <typename T> class EngineImpl final : public Engine {
         UPDC_CUDA(cudaMemcpy(dh, th.data(), th.size() * sizeof(cx<D>), cudaMemcpyHostToDevice));
         pm.tw = dm;
         ph.tw = dh;
-        FftPlan *dpm = dalloc<FftPlan>(1, nullptr), *dph = dalloc<FftPlan>(1, nullptr);
-        UPDC_CUDA(cudaMemcpy(dpm, &pm, sizeof(FftPlan), cudaMemcpyHostToDevice));
-        UPDC_CUDA(cudaMemcpy(dph, &ph, sizeof(FftPlan), cudaMemcpyHostToDevice));
         std::vector<cx<D>> post(M_ + 1);
         const double two_pi = 6.283185307179586476925286766559;
         for (int u = 0; u <= M_; ++u) post[u] = cx<D>{std::cos(-two_pi * u / FW_), std::sin(-two_pi * u / FW_)};
         cx<D> *dpost = dalloc<cx<D>>(M_ + 1, nullptr);
         UPDC_CUDA(cudaMemcpy(dpost, post.data(), post.size() * sizeof(cx<D>), cudaMemcpyHostToDevice));
         cx<D> *kd = dalloc<cx<D>>(nexp_ * nu * FH_, nullptr);
-        psf_spectra<D>(kd, true, dpm, dph, pm, ph, dpost);
+        psf_spectra<D>(kd, true, pm, ph, dpost);
         D *sc = dalloc<D>(nexp_ * nout_, nullptr);
         dim3 grid((unsigned)std::min<size_t>(ceil_div(nout_, 256), 148 * 8), (unsigned)nexp_);
         k_scatter_t<T, D, T><<<grid, 256, 0, stream_>>>(d_exps_, nin_, nout_, (const T *)nullptr, 1, sc);
@@ -1083,7 +1071,7 @@ template <typename T> class EngineImpl final : public Engine {
         {
             dim3 g((unsigned)ceil_div(H_, B), (unsigned)nexp_);
             k_row_r2c<D, NT, Caps<D>::ROW, PlaneLoader<D>, false><<<g, NT, rsm, stream_>>>(
-                dpm, dpost, PlaneLoader<D>{sc, W_, nout_}, W_, H_, B, SpecRef{rs, H_, nu * H_}, no_map_);
+                pm, dpost, PlaneLoader<D>{sc, W_, nout_}, W_, H_, B, FastDiv((uint32_t)B), SpecRef{rs, H_, nu * H_}, no_map_);
         }
         const size_t b = fft_buf_bytes(FH_, sizeof(cx<D>), ph.pad_shift);
         const bool aux_needed = b + align16(FH_ * sizeof(cx<D>)) > SMEM_LIMIT;
@@ -1091,21 +1079,21 @@ template <typename T> class EngineImpl final : public Engine {
         const size_t s = aux_needed ? b : b + align16(FH_ * sizeof(cx<D>));
         if (FH_ <= Caps<D>::COL_S) {
             set_smem(k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_S>, s);
-            k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_S><<<(unsigned)nu, NtAdj<D>::value, s, stream_>>>(dph, rs, H_, nu * H_, H_, kd, nu * FH_, nexp_, cr, H_, H_, aux);
+            k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_S><<<(unsigned)nu, NtAdj<D>::value, s, stream_>>>(ph, rs, H_, nu * H_, H_, kd, nu * FH_, nexp_, cr, H_, H_, aux);
         } else {
             set_smem(k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_L>, s);
-            k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_L><<<(unsigned)nu, NtAdj<D>::value, s, stream_>>>(dph, rs, H_, nu * H_, H_, kd, nu * FH_, nexp_, cr, H_, H_, aux);
+            k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_L><<<(unsigned)nu, NtAdj<D>::value, s, stream_>>>(ph, rs, H_, nu * H_, H_, kd, nu * FH_, nexp_, cr, H_, H_, aux);
         }
         D *den = dalloc<D>(nout_, nullptr);
         set_smem(k_row_c2r<D, NT, Caps<D>::ROW, PlaneStore<D>, false>, rsm);
         dim3 g2((unsigned)ceil_div(H_, B), 1);
         k_row_c2r<D, NT, Caps<D>::ROW, PlaneStore<D>, false><<<g2, NT, rsm, stream_>>>(
-            dpm, dpost, SpecRef{cr, H_, 0}, no_map_, H_, W_, B, 1.0 / (double)((size_t)FW_ * FH_),
+            pm, dpost, SpecRef{cr, H_, 0}, no_map_, H_, W_, B, FastDiv((uint32_t)B), 1.0 / (double)((size_t)FW_ * FH_),
             PlaneStore<D>{den, W_, 0}, d_err_);
         k_convert<D, T><<<grid1d(nout_), 256, 0, stream_>>>(den, den_, nout_);
         UPDC_CUDA(cudaGetLastError());
         UPDC_CUDA(cudaStreamSynchronize(stream_));
-        for (void *p : {(void *)dm, (void *)dh, (void *)dpm, (void *)dph, (void *)dpost, (void *)kd, (void *)sc, (void *)rs, (void *)cr, (void *)aux, (void *)den})
+        for (void *p : {(void *)dm, (void *)dh, (void *)dpost, (void *)kd, (void *)sc, (void *)rs, (void *)cr, (void *)aux, (void *)den})
             if (p) cudaFree(p);
     }
 

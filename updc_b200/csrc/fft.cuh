@@ -376,46 +376,25 @@ template <int R, int NT, int CAP> struct StageK {
     static constexpr int value = (CAP / R + NT - 1) / NT;
 };
 
-__device__ __forceinline__ FastDiv FastDiv_v(const volatile FastDiv &v) {
-    FastDiv r;
-    r.d = v.d;
-    r.mul = v.mul;
-    r.shift = v.shift;
-    return r;
-}
-
-// Copies a plan from device memory into the block's shared copy.  Kernels
-// keep the plan in shared memory: indexing a kernel-parameter array
-// dynamically would force a local copy of the structure, and reading the
-// fields from global memory on every stage exposes a full memory latency.
-__device__ __forceinline__ void load_plan(const FftPlan *__restrict__ g, FftPlan *s) {
-    const int *src = reinterpret_cast<const int *>(g);
-    int *dst = reinterpret_cast<int *>(s);
-    for (int i = threadIdx.x; i < (int)(sizeof(FftPlan) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
-    __syncthreads();
-}
-
 // Transforms `batch` sequences of length plan.n stored back to back (logical
 // index b*n + i, shared-memory slot fpad(., plan.pad_shift)) in buf (batch * n <= CAP).
-// Every thread of the block must call this; `plan` points to the block's
-// shared copy, whose radices must not exceed RMAX.  Stages run in descending
-// radix order (fft_factor), one loop per radix, so that only one radix's
-// registers are live at a time (a single switch inside one loop makes ptxas
-// spill).
+// Every thread of the block must call this; `plan` is the kernel's
+// __grid_constant__ parameter, so its per-stage fields are read from the
+// constant bank with a block-uniform index (no shared or local copy, nothing
+// held in registers across the callers' loops).  Radices must not exceed
+// RMAX.  Stages run in descending radix order (fft_factor), one loop per
+// radix, so that only one radix's registers are live at a time (a single
+// switch inside one loop makes ptxas spill).
 template <bool INV, int NT, int CAP, int RMAX, typename T>
-__device__ __forceinline__ void fft_batch(cx<T> *buf, int batch, const FftPlan *plan) {
-    // volatile (shared-memory) reads keep the per-stage fields from being
-    // hoisted out of the callers' loops (a hoisted copy of the whole plan
-    // would spill)
-    const volatile FftPlan *vp = plan;
-    const cx<T> *tw = reinterpret_cast<const cx<T> *>(vp->tw);
-    const int n = vp->n, nstage = vp->nstage, sh = vp->pad_shift;
+__device__ __forceinline__ void fft_batch(cx<T> *buf, int batch, const FftPlan &plan) {
+    const cx<T> *tw = reinterpret_cast<const cx<T> *>(plan.tw);
+    const int n = plan.n, nstage = plan.nstage, sh = plan.pad_shift;
     int s = 0;
 #define UPDC_FFT_RUN(R)                                                                                     \
     if constexpr (R <= RMAX) {                                                                             \
-        _Pragma("unroll 1") while (s < nstage && vp->radix[s] == R) {                                      \
-            fft_stage<R, StageK<R, NT, CAP>::value, INV, NT>(buf, n, batch, vp->ns[s], FastDiv_v(vp->ns_div[s]), \
-                                                             FastDiv_v(vp->nb_div[s]), tw + vp->twoff[s], sh); \
+        _Pragma("unroll 1") while (s < nstage && plan.radix[s] == R) {                                     \
+            fft_stage<R, StageK<R, NT, CAP>::value, INV, NT>(buf, n, batch, plan.ns[s], plan.ns_div[s],         \
+                                                             plan.nb_div[s], tw + plan.twoff[s], sh);           \
             ++s;                                                                                           \
         }                                                                                                  \
     }

@@ -81,13 +81,11 @@ __host__ __device__ inline size_t row_stage_bytes(int B, int M, size_t csize) {
 // blockIdx.y.
 template <typename T, int NT, int CAP, class Loader, bool TMA>
 __global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
-    k_row_r2c(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ post, Loader ld, int W, int rows, int B,
-              SpecRef out, const __grid_constant__ CUtensorMap omap) {
+    k_row_r2c(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ post, Loader ld, int W, int rows, int B,
+              FastDiv bdiv, SpecRef out, const __grid_constant__ CUtensorMap omap) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
-    __shared__ FftPlan s_plan;
-    load_plan(plan, &s_plan);
-    const int M = s_plan.n, sh = s_plan.pad_shift;
+    const int M = plan.n, sh = plan.pad_shift;
     const int y0 = blockIdx.x * B;
     const int nb = min(B, rows - y0);
     const int kexp = blockIdx.y;
@@ -102,12 +100,12 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
             buf[fpad(b * M + m, sh)] = {a, c};
         }
     __syncthreads();
-    fft_batch<false, NT, CAP, FFT_RMAX>(buf, B, &s_plan);
+    fft_batch<false, NT, CAP, FFT_RMAX>(buf, B, plan);
     cx<T> *stage = reinterpret_cast<cx<T> *>(smem_raw + row_buf_bytes(B, M, sizeof(cx<T>), sh));
     cx<T> *dst = reinterpret_cast<cx<T> *>(out.p) + kexp * out.batch_stride;
     const T half = T(0.5);
     for (int i = threadIdx.x; i < (M + 1) * B; i += NT) {
-        const int u = i / B, b = i - u * B;
+        const int u = (int)bdiv.div((uint32_t)i), b = i - u * B;
         cx<T> X = {0, 0};
         if (b < nb) {
             const cx<T> Z = buf[fpad(b * M + (u == M ? 0 : u), sh)];
@@ -150,15 +148,13 @@ template <typename T> struct PlaneStore {
 // With TMA the block's {B rows} x {all u} tile arrives through the tensor map.
 template <typename T, int NT, int CAP, class Epi, bool TMA>
 __global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
-    k_row_c2r(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ post, SpecRef in,
-              const __grid_constant__ CUtensorMap imap, int rows, int W, int B, T scale, Epi epi,
+    k_row_c2r(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ post, SpecRef in,
+              const __grid_constant__ CUtensorMap imap, int rows, int W, int B, FastDiv bdiv, T scale, Epi epi,
               unsigned long long *__restrict__ err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
-    __shared__ FftPlan s_plan;
     __shared__ __align__(8) uint64_t bar;
-    load_plan(plan, &s_plan);
-    const int M = s_plan.n, sh = s_plan.pad_shift;
+    const int M = plan.n, sh = plan.pad_shift;
     const int y0 = blockIdx.x * B;
     const int nb = min(B, rows - y0);
     const int kexp = blockIdx.y;
@@ -181,7 +177,7 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
         }
     }
     for (int i = threadIdx.x; i < M * B; i += NT) {
-        const int k = i / B, b = i - k * B;
+        const int k = (int)bdiv.div((uint32_t)i), b = i - k * B;
         cx<T> Zp = {0, 0};
         if (b < nb) {
             cx<T> X, Xm;
@@ -202,7 +198,7 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
         buf[fpad(b * M + k, sh)] = Zp;
     }
     __syncthreads();
-    fft_batch<true, NT, CAP, FFT_RMAX>(buf, B, &s_plan);
+    fft_batch<true, NT, CAP, FFT_RMAX>(buf, B, plan);
     for (int b = 0; b < nb; ++b)
         for (int x = threadIdx.x; x < W; x += NT) {
             const cx<T> z = buf[fpad(b * M + (x >> 1), sh)];
@@ -220,15 +216,13 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
 // conj(FFT(conj(.))), which keeps a single inlined copy of the FFT (two
 // copies make ptxas spill).
 template <typename T, int NT, int CAP>
-__global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_forward(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ rx, int ldr, int rows_in,
+__global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_forward(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ rx, int ldr, int rows_in,
                                                     const cx<T> *__restrict__ khat, size_t khat_stride, int nexp,
                                                     cx<T> *__restrict__ y, int ldy, size_t y_stride, int rows_out,
                                                     int nu, cx<T> *aux) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
-    __shared__ FftPlan s_plan;
-    load_plan(plan, &s_plan);
-    const int n = s_plan.n, sh = s_plan.pad_shift;
+    const int n = plan.n, sh = plan.pad_shift;
     const int u = blockIdx.x;
     cx<T> *xh = aux ? aux + (size_t)u * n : reinterpret_cast<cx<T> *>(smem_raw + fft_buf_bytes(n, sizeof(cx<T>), sh));
     const cx<T> *src = rx + (size_t)u * ldr;
@@ -244,7 +238,7 @@ __global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_forw
             }
         }
         __syncthreads();
-        fft_batch<false, NT, CAP, FFT_RMAX>(buf, 1, &s_plan);
+        fft_batch<false, NT, CAP, FFT_RMAX>(buf, 1, plan);
         if (it == 0) {
             for (int v = threadIdx.x; v < n; v += NT) xh[v] = buf[fpad(v, sh)];
         } else {
@@ -305,14 +299,12 @@ struct AccKahan {  // FP32 products, Kahan-compensated FP32 sum
 // the final inverse goes through the same forward-FFT call site as
 // conj(FFT(conj(.))).
 template <typename T, class Acc, int NT, int CAP>
-__global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_adjoint(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ rs, int ldr, size_t rs_stride,
+__global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_adjoint(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ rs, int ldr, size_t rs_stride,
                                                     int rows_in, const cx<T> *__restrict__ khat, size_t khat_stride, int nexp,
                                                     cx<T> *__restrict__ c, int ldc, int rows_out, typename Acc::S *aux) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
-    __shared__ FftPlan s_plan;
-    load_plan(plan, &s_plan);
-    const int n = s_plan.n, sh = s_plan.pad_shift;
+    const int n = plan.n, sh = plan.pad_shift;
     const int u = blockIdx.x;
     typename Acc::S *acc = aux ? aux + (size_t)u * n
                                : reinterpret_cast<typename Acc::S *>(smem_raw + fft_buf_bytes(n, sizeof(cx<T>), sh));
@@ -329,7 +321,7 @@ __global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_adjo
             }
         }
         __syncthreads();
-        fft_batch<false, NT, CAP, FFT_RMAX>(buf, 1, &s_plan);
+        fft_batch<false, NT, CAP, FFT_RMAX>(buf, 1, plan);
         if (it < nexp) {
             const cx<T> *kr = khat + it * khat_stride + (size_t)u * n;
             for (int v = threadIdx.x; v < n; v += NT) Acc::add(acc[v], buf[fpad(v, sh)], kr[v]);
@@ -346,18 +338,16 @@ __global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_adjo
 
 // Plain column transform (setup: PSF spectra and generic 2-D transforms).
 template <typename T, int NT, int CAP, bool INV>
-__global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_fft(const FftPlan *__restrict__ plan, const cx<T> *__restrict__ in, int ldi, int rows_in,
+__global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_fft(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ in, int ldi, int rows_in,
                                                 cx<T> *__restrict__ out, int ldo, int rows_out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
-    __shared__ FftPlan s_plan;
-    load_plan(plan, &s_plan);
-    const int n = s_plan.n, sh = s_plan.pad_shift;
+    const int n = plan.n, sh = plan.pad_shift;
     const int u = blockIdx.x;
     const cx<T> *src = in + (size_t)u * ldi;
     for (int v = threadIdx.x; v < n; v += NT) buf[fpad(v, sh)] = v < rows_in ? src[v] : cx<T>{0, 0};
     __syncthreads();
-    fft_batch<INV, NT, CAP, FFT_RMAX>(buf, 1, &s_plan);
+    fft_batch<INV, NT, CAP, FFT_RMAX>(buf, 1, plan);
     cx<T> *dst = out + (size_t)u * ldo;
     for (int v = threadIdx.x; v < rows_out; v += NT) dst[v] = buf[fpad(v, sh)];
 }

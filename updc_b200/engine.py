@@ -68,6 +68,7 @@ class Engine:
         self.form = form
         self.dtype = np.float64 if form == "fp64" else np.float32
         self.W = self.H = self.iw = self.ih = self.nexp = 0
+        self.iterations_done = 0
 
     def close(self) -> None:
         if self._h:
@@ -105,6 +106,7 @@ class Engine:
         mn = np.zeros((n, self.nexp), np.float64)
         check(self._L.updc_iterate(self._h, n, 1 if check_each else 0, st, new.ctypes.data,
                                    tot.ctypes.data, mn.ctypes.data))
+        self.iterations_done += n
         return [IterationStats(st[i].seconds, st[i].signed_sum, int(st[i].negative), new[i], tot[i], mn[i],
                                np.array(st[i].stage_seconds[:])) for i in range(n)]
 
