@@ -100,6 +100,35 @@ int updc_stage_detector(updc_engine *h, uint64_t *new_frozen, uint64_t *total_fr
 int updc_stage_correction(updc_engine *h);
 int updc_stage_update(updc_engine *h, double *signed_sum, uint64_t *negative);
 
+/* The update x *= C/D (updc_stage_update's kernels and grid) on caller-owned
+ * FP32 device planes of n pixels, for callers that may not allocate device
+ * memory at this point: an allocator-managed pool, a real-time or
+ * memory-capped host process, a caller holding its own memory pool.  No
+ * counterpart in the reference, whose update is a host loop on its own
+ * buffers (updc_core.c:1437-1456).
+ *   - allocates nothing: no cudaMalloc/cudaFree, no allocating library call;
+ *     its scratch is one file-scope __device__ array of
+ *     UPDC_UPDATE_NOALLOC_SCRATCH_BYTES bytes per device;
+ *   - the first call on each device looks the scratch up with
+ *     cudaGetSymbolAddress; make that first call before any stream capture
+ *     begins on the device;
+ *   - nothing in the scratch has to start at zero: each call first sets the
+ *     error record to "none", and every partial slot is written before it is
+ *     read;
+ *   - the scratch is shared by every call on a device, so calls that overlap
+ *     in time (other streams or threads) race; order them on one stream or
+ *     serialise them on the host;
+ *   - n must be 1 .. UPDC_UPDATE_NOALLOC_MAX_PIXELS (the width of the device
+ *     error record's pixel index); other sizes return status 1 with a message;
+ *   - runs on the current device and on `stream` (a cudaStream_t; NULL for the
+ *     legacy default stream), waits for it, and returns the signed sum and the
+ *     negative count of the updated estimate, or the reference's failure
+ *     message through updc_last_error(). */
+#define UPDC_UPDATE_NOALLOC_SCRATCH_BYTES ((size_t)(16 * 148 * 16 + 24))
+#define UPDC_UPDATE_NOALLOC_MAX_PIXELS ((uint64_t)1 << 40)
+int updc_update_noalloc(const float *correction, const float *denominator, float *estimate, uint64_t n,
+                        float max_sensitivity, void *stream, double *signed_sum, uint64_t *negative);
+
 /* LinkMap v2 (updc_core.c:40-79, 463-496, 530-609, 645-662). */
 uint64_t updc_link_count(updc_engine *h, int exposure);
 int updc_link_encoding(updc_engine *h, int exposure);

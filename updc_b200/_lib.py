@@ -70,6 +70,7 @@ def load() -> ctypes.CDLL:
     L.updc_stage_detector.argtypes = [P, P, P, P]
     L.updc_stage_correction.argtypes = [P]
     L.updc_stage_update.argtypes = [P, c.POINTER(c.c_double), c.POINTER(c.c_uint64)]
+    L.updc_update_noalloc.argtypes = [P, P, P, c.c_uint64, c.c_float, P, c.POINTER(c.c_double), c.POINTER(c.c_uint64)]
     L.updc_link_count.restype = c.c_uint64
     L.updc_link_count.argtypes = [P, c.c_int]
     L.updc_link_encoding.argtypes = [P, c.c_int]

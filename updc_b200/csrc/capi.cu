@@ -193,6 +193,14 @@ int updc_decode_links(updc_engine *h, int k, uint32_t *targets) {
     return guarded([&] { h->e->decode_links(k, targets); });
 }
 
+int updc_update_noalloc(const float *correction, const float *denominator, float *estimate, uint64_t n,
+                        float max_sensitivity, void *stream, double *signed_sum, uint64_t *negative) {
+    return guarded([&] {
+        update_noalloc(correction, denominator, estimate, n, max_sensitivity, static_cast<cudaStream_t>(stream),
+                       signed_sum, negative);
+    });
+}
+
 int updc_build_linkmap(const char *vertices, const char *links, int iw, int ih, int W, int H, uint64_t *nlinks,
                        int *encoding) {
     return guarded([&] {

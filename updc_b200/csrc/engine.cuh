@@ -82,4 +82,9 @@ std::unique_ptr<Engine> make_engine(const EngineOptions &opt);
 // Smallest even / any 7-smooth integer >= n.
 int next_smooth(int n, bool even);
 
+// The update on caller-owned FP32 device planes with file-scope scratch
+// (noalloc.cu); throws Error with the reference's message on failure.
+void update_noalloc(const float *correction, const float *denominator, float *estimate, uint64_t n,
+                    float max_sensitivity, cudaStream_t stream, double *signed_sum, uint64_t *negative);
+
 }  // namespace updc

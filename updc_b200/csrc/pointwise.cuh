@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(256) k_update(size_t nout, const T *__restrict
 }
 
 // Fixed-order final reduction of per-block partials (deterministic).
-__global__ void k_reduce_partials(const double *part_sum, const unsigned long long *part_neg, int n, double *out_sum,
+static __global__ void k_reduce_partials(const double *part_sum, const unsigned long long *part_neg, int n, double *out_sum,
                                   unsigned long long *out_neg) {
     __shared__ double s[256];
     __shared__ unsigned long long c[256];
@@ -361,7 +361,7 @@ __global__ void k_weight_norm(size_t nin, const float *__restrict__ sci_raw, con
 }
 
 // Every 64th weight of one exposure, finite and > 0 (updc_core.c:380-384).
-__global__ void k_weight_sample(size_t nin, const float *__restrict__ wht_raw, float *__restrict__ out,
+static __global__ void k_weight_sample(size_t nin, const float *__restrict__ wht_raw, float *__restrict__ out,
                                 unsigned int *__restrict__ count) {
     for (size_t p = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) * 64; p < nin; p += (size_t)gridDim.x * blockDim.x * 64) {
         const float w = wht_raw[p];
@@ -373,7 +373,7 @@ __global__ void k_weight_sample(size_t nin, const float *__restrict__ wht_raw, f
 }
 
 // PSF validity and FP64 sum (fixed-order block tree; deterministic).
-__global__ void k_psf_sum_f64(const float *__restrict__ psf, size_t n, double *__restrict__ partial,
+static __global__ void k_psf_sum_f64(const float *__restrict__ psf, size_t n, double *__restrict__ partial,
                               unsigned long long *__restrict__ err) {
     __shared__ double s[256];
     double a = 0.0;
@@ -393,7 +393,7 @@ __global__ void k_psf_sum_f64(const float *__restrict__ psf, size_t n, double *_
 
 // Neumaier float sum in the reference's serial order (updc_core.c:777-789),
 // for the reference-precision form.  One thread; setup only.
-__global__ void k_psf_sum_neumaier(const float *__restrict__ psf, size_t n, float *__restrict__ out,
+static __global__ void k_psf_sum_neumaier(const float *__restrict__ psf, size_t n, float *__restrict__ out,
                                    unsigned long long *__restrict__ err) {
     if (threadIdx.x || blockIdx.x) return;
     float sum = 0.0f, comp = 0.0f;

@@ -212,6 +212,18 @@ def build_linkmap(vertices: str, links: str, input_width: int, input_height: int
     return int(nl.value), int(enc.value)
 
 
+def update_noalloc(correction: int, denominator: int, estimate: int, n: int, max_sensitivity: float,
+                   stream: int = 0):
+    """x *= C/D on caller-owned FP32 device planes (addresses as ints) with no
+    device allocation; returns (signed_sum, negative).  Calls that overlap in
+    time on one device race on the shared scratch."""
+    s = ctypes.c_double()
+    neg = ctypes.c_uint64()
+    check(_lib.load().updc_update_noalloc(correction, denominator, estimate, n, max_sensitivity, stream or None,
+                                          ctypes.byref(s), ctypes.byref(neg)))
+    return float(s.value), int(neg.value)
+
+
 def polygon_area(points: np.ndarray) -> float:
     p = np.ascontiguousarray(points, np.float64)
     return float(_lib.load().updc_polygon_area(p.ctypes.data, len(p)))
