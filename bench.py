@@ -274,7 +274,7 @@ def b200_arm(args, rank, world, local_rank):
     w = synth.WORKLOADS[args.workload]
     workdir = Path(args.data_dir or tempfile.mkdtemp(prefix=f"updc_bench_r{rank}_"))
     ds = synth.generate(w.name, workdir, use_torch=True)
-    eng = Engine(form=args.form, device=local_rank)
+    eng = Engine(form=args.form, device=local_rank, autotune=not args.no_autotune, tune_cache_dir=workdir)
     eng.load(str(ds.manifest), w.W, w.H, w.iw, w.ih, w.nexp)
     t0 = time.time()
     eng.setup()
@@ -334,11 +334,14 @@ def b200_arm(args, rank, world, local_rank):
         "data": "synthetic",
         "config": {"workload": args.workload, "form": args.form, "target": [w.W, w.H], "exposures": w.nexp,
                    "detector": [w.iw, w.ih], "psf": w.psf_size, "fft": [fw, fh],
+                   "fft_radices": {"rows": eng.fft_radices(0), "columns": eng.fft_radices(1)},
+                   "autotune": None if args.no_autotune else eng.autotune_info,
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "working set ~%.1f GB >> 126 MB L2; no flush needed" % (eng.device_bytes / 1e9)},
         "wall_ms_per_step": round(1000.0 * wall / args.steps, 4),
         "setup_s": round(setup_s, 2),
         "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+        "stage_gbs": {k: round(sb[k] / (stage_ms[k] * 1e-3) / 1e9, 1) for k in STAGES},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                      "algorithmic_bytes": sb[dom], "traffic": None},
@@ -372,6 +375,8 @@ def main():
     p.add_argument("--form", default="fp32", choices=["fp32", "fp64", "fp32-kahan", "fp32-reference"])
     p.add_argument("--data-dir", default=None)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="smallest 7-smooth FFT shape and greedy radix splits instead of the device autotuner")
     p.add_argument("--no-fp64-check", action="store_true",
                    help="skip the FP64-form run that gives the metric's accuracy side")
     args = p.parse_args()

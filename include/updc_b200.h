@@ -48,6 +48,10 @@ typedef struct {
     int fft_width;       /* 0: smallest even 7-smooth >= W + pw - 1 */
     int fft_height;      /* 0: smallest 7-smooth >= H + ph - 1 */
     int stage_timing;    /* per-stage CUDA-event timing (disables the graph) */
+    int autotune;        /* time candidate FFT shapes and radix splits on the device at setup
+                            (select_fft_shape, updc_core.c:242-291) */
+    int retune;          /* ignore a cached autotune choice */
+    const char *tune_cache_dir; /* directory of the autotune cache; NULL or "" = none */
 } updc_options;
 
 typedef struct {
@@ -83,8 +87,14 @@ int updc_iterate(updc_engine *h, int n, int check_each, updc_iter_stats *stats, 
 int updc_read_plane(updc_engine *h, int which, int exposure, void *host, int as_double);
 int updc_write_plane(updc_engine *h, int which, int exposure, const void *host, int as_double);
 /* Scalars: 0 weight_scale, 1 max_sensitivity, 2 FFT width, 3 FFT height, 4 masked pixels,
- * 5 working precision bits, 6 compensated raw_mu flag. */
+ * 5 working precision bits, 6 compensated raw_mu flag, 7 FFT autotune seconds,
+ * 8 FFT plans timed by the autotuner, 9 autotune cache hit, 10 modelled spectral
+ * ms per iteration of the tuned choice. */
 double updc_scalar(updc_engine *h, int which);
+/* Radix split of an FFT axis (0: the row transform of FW/2 points, 1: the
+ * column transform of FH points) in stage order; *count receives the number
+ * of stages (at most `capacity` are written). */
+int updc_fft_radices(updc_engine *h, int axis, int *radices, int capacity, int *count);
 /* Per-stage CUDA-event timing of the following iterations (on: eager launches, no graph). */
 int updc_set_stage_timing(updc_engine *h, int on);
 size_t updc_device_bytes(updc_engine *h);
@@ -129,6 +139,35 @@ int updc_stage_update(updc_engine *h, double *signed_sum, uint64_t *negative);
 int updc_update_noalloc(const float *correction, const float *denominator, float *estimate, uint64_t n,
                         float max_sensitivity, void *stream, double *signed_sum, uint64_t *negative);
 
+/* Differentiable model (no reference counterpart; the gradient of the
+ * weighted Poisson negative log-likelihood whose multiplicative update the
+ * reference runs, updc_core.c:1140-1183, 1437-1456):
+ *   mu_k = S_k P_k x + background_k + pedestal_k,  y_k = SCI_k + pedestal_k,
+ *   L = sum_k sum_p W_kp (mu_kp - y_kp log mu_kp)  over pixels with W > 0, mu > 0.
+ * updc_set_exposure_offsets / updc_set_psf replace one exposure's background
+ * and pedestal, or its PSF (FP32, or FP64 with as_double, manifest layout, no
+ * larger than the PSF the FFT shape was chosen for; normalised by its sum
+ * like core:777-843).
+ * updc_nll runs the forward model of the current estimate and writes per
+ * exposure 4 doubles {L_k, sum r, sum W log mu, pixels left out} with
+ * r = W (1 - y/mu) kept in the WR planes; updc_nll_adjoint then leaves
+ * dL/dx = sum_k H_k^T r_k in the CORRECTION plane; updc_psf_gradient gives
+ * dL/dpsi for the normalised PSF of one exposure (psf_width x psf_height
+ * doubles, PSF layout).  updc_copy_plane_device copies a plane to or from
+ * caller device memory (to_engine = 1 writes the plane) after `stream`. */
+int updc_set_exposure_offsets(updc_engine *h, int exposure, double background, double pedestal);
+int updc_set_psf(updc_engine *h, int exposure, const void *psf, int psf_width, int psf_height, int as_double);
+int updc_nll(updc_engine *h, double *terms);
+/* The FP64 per-block partial sums behind the last updc_nll (exposures x
+ * blocks x 4, the terms' order); *count receives their number.  Differences
+ * of two evaluations taken partial by partial are exact where nothing
+ * changed (finite differences of single pixels). */
+int updc_nll_partials(updc_engine *h, double *out, size_t capacity, size_t *count);
+int updc_nll_adjoint(updc_engine *h);
+int updc_psf_gradient(updc_engine *h, int exposure, double *out);
+int updc_copy_plane_device(updc_engine *h, int which, int exposure, void *device_ptr, int to_engine, int as_double,
+                           void *stream);
+
 /* LinkMap v2 (updc_core.c:40-79, 463-496, 530-609, 645-662). */
 uint64_t updc_link_count(updc_engine *h, int exposure);
 int updc_link_encoding(updc_engine *h, int exposure);
@@ -137,6 +176,32 @@ int updc_decode_links(updc_engine *h, int exposure, uint32_t *targets);
 /* Build a LinkMap file from a vertex map on the GPU (AreaLinkList_O2TAD_stream, updc_core.c:530-609). */
 int updc_build_linkmap(const char *vertices_path, const char *links_path, int input_width, int input_height,
                        int width, int height, uint64_t *nlinks, int *encoding);
+
+/* Batched fields (no reference counterpart: the reference solves one field
+ * per process).  Many independent fields of uneven grid size and exposure
+ * count, each with its own manifest, FFT shape (autotuned when opt->autotune)
+ * and LinkMaps, iterate together: every stage of an iteration is one
+ * persistent launch over the work units of all fields, and n iterations
+ * without per-iteration checks run as one CUDA graph.  Each field computes
+ * exactly what its own engine computes (updc_core.c:1410-1456 per field).
+ * updc_batch_iterate fills, per iteration i, seconds[i] (device time of the
+ * whole batch), signed_sum/negative[i * fields + f] and
+ * total_frozen[i * E + e] (E = all exposures, fields in order); any may be
+ * NULL.  updc_batch_field returns a handle owned by the batch for the plane
+ * and scalar queries of one field (do not destroy it). */
+typedef struct updc_batch updc_batch;
+int updc_batch_create(const updc_options *opt, updc_batch **out);
+int updc_batch_destroy(updc_batch *b);
+int updc_batch_add_field(updc_batch *b, const char *manifest, int width, int height, int input_width,
+                         int input_height, int exposures, int psf_transposed);
+int updc_batch_setup(updc_batch *b);
+int updc_batch_fields(updc_batch *b);
+updc_engine *updc_batch_field(updc_batch *b, int field);
+/* Work units of a stage (0 estimate rows, 1 columns, 2 forward rows, 3 detector,
+ * 4 adjoint gather, 5 scatter rows, 6 update, 7 adjoint rows). */
+size_t updc_batch_units(updc_batch *b, int stage);
+int updc_batch_iterate(updc_batch *b, int n, int check_each, double *seconds, double *signed_sum, uint64_t *negative,
+                       uint64_t *total_frozen);
 
 /* Geometry (overlap.c:72-116) and the known-answer self-test (updc_core.c:1545-1564). */
 float updc_polygon_area(const double *xy, int count);

@@ -65,6 +65,7 @@ def lib() -> ctypes.CDLL:
         L.orc_detector.argtypes = [c.c_void_p, c.c_int, c.c_void_p, c.c_void_p, c.POINTER(c.c_uint64),
                                    c.POINTER(c.c_uint64), c.POINTER(c.c_double), c.c_char_p, c.c_int]
         L.orc_update.argtypes = [c.c_void_p, c.c_char_p, c.c_int]
+        L.orc_adjoint.argtypes = [c.c_void_p, c.c_void_p, c.c_void_p]
         L.orc_fft_r2c.argtypes = [c.c_int] * 4 + [c.c_void_p, c.c_void_p]
         L.orc_fft_c2r.argtypes = [c.c_int] * 4 + [c.c_void_p, c.c_void_p]
         _lib = L
@@ -211,6 +212,15 @@ class Solver:
                               ctypes.byref(mm), err, 512):
             raise RuntimeError("UPDC_ALL: " + err.value.decode())
         return out, int(nn.value), int(nt.value), float(mm.value)
+
+    def adjoint(self, v: np.ndarray) -> np.ndarray:
+        """H^T v for detector planes v (nexp x ih x iw) with the reference's
+        scatter and frequency-domain adjoint (updc_core.c:988-995, 1175-1176,
+        1280-1287); returns the target plane."""
+        a = np.ascontiguousarray(v, dtype=self.dtype)
+        out = np.zeros((self.H, self.W), self.dtype)
+        lib().orc_adjoint(self.h, a.ctypes.data, out.ctypes.data)
+        return out
 
 
 def fft_r2c(x: np.ndarray, precision: int = 64, nthreads: int = 4) -> np.ndarray:

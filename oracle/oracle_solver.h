@@ -184,6 +184,31 @@ static int OR_NS(denominator_stage)(OR_NS(solver) *s) {
     return 0;
 }
 
+/* H^T v = crop(C2R(sum_k conj(K_k) R2C(pad(S_k^T v_k))))/nf for detector
+ * planes v (nexp x nin): the scatter of core:1175-1176 (fmaf in link order),
+ * the adjoint accumulation of core:988-995 and the reduction of
+ * core:1280-1287, applied to arbitrary detector values (the differentiable
+ * model's residual W(ratio - 1)).  Result in dest (nout). */
+static void OR_NS(adjoint)(OR_NS(solver) *s, const OR_REAL *v_all, OR_REAL *dest) {
+    memset(s->partial, 0, 2 * s->nc * sizeof(OR_REAL));
+    for (int k = 0; k < s->nexp; ++k) {
+        const OR_REAL *v = v_all + (size_t)k * s->nin;
+        const uint32_t *off = s->offset[k], *tg = s->target[k];
+        const float *fr = s->frac[k];
+        memset(s->scatter, 0, s->nout * sizeof(OR_REAL));
+        for (size_t p = 0; p < s->nin; ++p) {
+            if (off[p] == off[p + 1]) continue;
+            const OR_REAL vp = v[p];
+            for (uint32_t z = off[p]; z < off[p + 1]; ++z)
+                s->scatter[tg[z]] = OR_FMA((OR_REAL)fr[z], vp, s->scatter[tg[z]]);
+        }
+        OR_NS(forward_target)(s, s->scatter, s->fft_freq);
+        OR_NS(accumulate_adjoint)(s, s->partial, s->fft_freq, s->spectrum[k]);
+    }
+    for (size_t p = 0; p < 2 * s->nc; ++p) s->fft_freq[p] = (OR_REAL)0 + s->partial[p];
+    OR_NS(inverse_crop)(s, dest);
+}
+
 /* core:1152-1177 fused detector loop of one exposure given its blur plane.
  * Writes scatter (zeroed first) and updates the freeze mask. */
 static int OR_NS(detector)(const OR_NS(solver) *s, int k, const OR_REAL *blur, OR_REAL *scatter,

@@ -556,6 +556,14 @@ int orc_detector(void *h, int k, const void *blur, void *scatter, uint64_t *nnew
     return rc;
 }
 
+/* H^T of detector planes v (nexp x nin, the solver's precision) into out
+ * (nout), with the reference's scatter and frequency-domain adjoint. */
+void orc_adjoint(void *h, const void *v, void *out) {
+    OHandle *hd = (OHandle *)h;
+    if (hd->precision == 64) orcd_adjoint((orcd_solver *)hd->s, (const double *)v, (double *)out);
+    else orcf_adjoint((orcf_solver *)hd->s, (const float *)v, (float *)out);
+}
+
 /* Update stage on the solver's correction plane (core:1437-1456). */
 int orc_update(void *h, char *err, int errcap) {
     OHandle *hd = (OHandle *)h;

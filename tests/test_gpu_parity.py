@@ -214,6 +214,28 @@ def test_graph_and_eager_paths_identical(engine_lib, datasets):
     np.testing.assert_array_equal(outs[0], outs[2])
 
 
+def test_whole_loop_graph_matches_per_iteration_launches(engine_lib, datasets):
+    """iterate(n) without per-iteration checks replays one graph of all n
+    iterations; its estimate and per-iteration records equal those of n
+    checked single-iteration launches."""
+    ds = datasets("c0", background=-100.0)        # FreezeMu counters change per iteration
+    a = _engine(ds, form="fp32")
+    b = _engine(ds, form="fp32")
+    ra = a.iterate(6, check_each=False)
+    rb = [b.iterate(1, check_each=True)[0] for _ in range(6)]
+    np.testing.assert_array_equal(a.plane("estimate"), b.plane("estimate"))
+    for x, y in zip(ra, rb):
+        assert x.signed_sum == y.signed_sum and x.negative == y.negative
+        np.testing.assert_array_equal(x.new_frozen, y.new_frozen)
+        np.testing.assert_array_equal(x.total_frozen, y.total_frozen)
+        assert x.seconds > 0
+    assert int(rb[-1].total_frozen.sum()) > 0
+    ra2 = a.iterate(6, check_each=False)          # the cached loop graph again
+    rb2 = [b.iterate(1, check_each=True)[0] for _ in range(6)]
+    np.testing.assert_array_equal(a.plane("estimate"), b.plane("estimate"))
+    assert [r.signed_sum for r in ra2] == [r.signed_sum for r in rb2]
+
+
 def test_dropin_executable(engine_lib, reference_binary, datasets, tmp_path):
     """updc_b200/bin/updc_jwst_c with the 18-argument contract writes the
     reference's outputs; the WHT product (coverage x weight scale) is

@@ -26,7 +26,8 @@ FORMS = {"fp32": FORM_FP32, "fp64": FORM_FP64, "fp32-kahan": FORM_FP32_KAHAN,
 class Options(ctypes.Structure):
     _fields_ = [("form", ctypes.c_int), ("compensated_mu", ctypes.c_int), ("use_graph", ctypes.c_int),
                 ("device", ctypes.c_int), ("reuse_links", ctypes.c_int), ("verbose", ctypes.c_int),
-                ("fft_width", ctypes.c_int), ("fft_height", ctypes.c_int), ("stage_timing", ctypes.c_int)]
+                ("fft_width", ctypes.c_int), ("fft_height", ctypes.c_int), ("stage_timing", ctypes.c_int),
+                ("autotune", ctypes.c_int), ("retune", ctypes.c_int), ("tune_cache_dir", ctypes.c_char_p)]
 
 
 class IterStats(ctypes.Structure):
@@ -66,11 +67,29 @@ def load() -> ctypes.CDLL:
     L.updc_device_bytes.restype = c.c_size_t
     L.updc_device_bytes.argtypes = [P]
     L.updc_set_stage_timing.argtypes = [P, c.c_int]
+    L.updc_fft_radices.argtypes = [P, c.c_int, P, c.c_int, c.POINTER(c.c_int)]
     L.updc_stage_forward.argtypes = [P]
     L.updc_stage_detector.argtypes = [P, P, P, P]
     L.updc_stage_correction.argtypes = [P]
     L.updc_stage_update.argtypes = [P, c.POINTER(c.c_double), c.POINTER(c.c_uint64)]
     L.updc_update_noalloc.argtypes = [P, P, P, c.c_uint64, c.c_float, P, c.POINTER(c.c_double), c.POINTER(c.c_uint64)]
+    L.updc_set_exposure_offsets.argtypes = [P, c.c_int, c.c_double, c.c_double]
+    L.updc_set_psf.argtypes = [P, c.c_int, P, c.c_int, c.c_int, c.c_int]
+    L.updc_nll.argtypes = [P, P]
+    L.updc_nll_partials.argtypes = [P, P, c.c_size_t, c.POINTER(c.c_size_t)]
+    L.updc_nll_adjoint.argtypes = [P]
+    L.updc_psf_gradient.argtypes = [P, c.c_int, P]
+    L.updc_copy_plane_device.argtypes = [P, c.c_int, c.c_int, P, c.c_int, c.c_int, P]
+    L.updc_batch_create.argtypes = [c.POINTER(Options), c.POINTER(P)]
+    L.updc_batch_destroy.argtypes = [P]
+    L.updc_batch_add_field.argtypes = [P, c.c_char_p] + [c.c_int] * 6
+    L.updc_batch_setup.argtypes = [P]
+    L.updc_batch_fields.argtypes = [P]
+    L.updc_batch_field.restype = P
+    L.updc_batch_field.argtypes = [P, c.c_int]
+    L.updc_batch_units.restype = c.c_size_t
+    L.updc_batch_units.argtypes = [P, c.c_int]
+    L.updc_batch_iterate.argtypes = [P, c.c_int, c.c_int, P, P, P, P]
     L.updc_link_count.restype = c.c_uint64
     L.updc_link_count.argtypes = [P, c.c_int]
     L.updc_link_encoding.argtypes = [P, c.c_int]

@@ -27,9 +27,9 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-r
               "-Xcompiler", "-Wall", "-I", str(ROOT / "include")]
 # geometry must not contract multiply-adds (bit-exact LinkMaps)
 PER_FILE = {"linkmap.cu": ["-fmad=false"]}
-SOURCES = ["linkmap.cu", "engine.cu", "capi.cu", "noalloc.cu"]
+SOURCES = ["linkmap.cu", "engine.cu", "capi.cu", "noalloc.cu", "batch.cu"]
 HEADERS = ["common.cuh", "fft.cuh", "kernels.cuh", "pointwise.cuh", "engine.cuh", "geometry.cuh", "linkmap.cuh",
-           "tma.cuh"]
+           "tma.cuh", "nll.cuh"]
 
 
 def nvcc() -> str:

@@ -1,6 +1,7 @@
 // C ABI of the B200 engine (include/updc_b200.h) and the UPDC_ALL driver.
 #include <sys/resource.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
@@ -15,9 +16,15 @@
 using namespace updc;
 
 struct updc_engine {
-    std::unique_ptr<Engine> e;
+    std::unique_ptr<Engine> owned;  // null for the field handles of a batch
+    Engine *e = nullptr;
     EngineOptions opt;
     int nexp = 0;
+};
+
+struct updc_batch {
+    std::unique_ptr<Batch> b;
+    std::vector<std::unique_ptr<updc_engine>> views;
 };
 
 namespace {
@@ -55,6 +62,9 @@ EngineOptions to_options(const updc_options *o) {
     r.fft_width = o->fft_width;
     r.fft_height = o->fft_height;
     r.stage_timing = o->stage_timing;
+    r.autotune = o->autotune;
+    r.retune = o->retune;
+    r.tune_cache_dir = o->tune_cache_dir ? o->tune_cache_dir : "";
     return r;
 }
 
@@ -79,6 +89,9 @@ void updc_default_options(updc_options *o) {
     o->fft_width = d.fft_width;
     o->fft_height = d.fft_height;
     o->stage_timing = d.stage_timing;
+    o->autotune = d.autotune;
+    o->retune = d.retune;
+    o->tune_cache_dir = nullptr;
 }
 
 int updc_create(const updc_options *opt, updc_engine **out) {
@@ -90,7 +103,8 @@ int updc_create(const updc_options *opt, updc_engine **out) {
         updc_engine *h = new updc_engine;
         h->opt = o;
         try {
-            h->e = make_engine(o);
+            h->owned = make_engine(o);
+            h->e = h->owned.get();
         } catch (...) {
             delete h;
             throw;
@@ -100,7 +114,10 @@ int updc_create(const updc_options *opt, updc_engine **out) {
 }
 
 int updc_destroy(updc_engine *h) {
-    return guarded([&] { delete h; });
+    return guarded([&] {
+        if (h && !h->owned) throw Error(1, "a batch field handle is owned by its batch");
+        delete h;
+    });
 }
 
 int updc_load_manifest(updc_engine *h, const char *manifest, int W, int H, int iw, int ih, int nexp, int tr) {
@@ -153,6 +170,15 @@ int updc_write_plane(updc_engine *h, int which, int k, const void *host, int as_
     });
 }
 double updc_scalar(updc_engine *h, int which) { return h ? h->e->scalar(which) : 0.0; }
+int updc_fft_radices(updc_engine *h, int axis, int *radices, int capacity, int *count) {
+    return guarded([&] {
+        if (!h) throw Error(1, "null handle");
+        const FftChoice &c = h->e->fft_choice();
+        const std::vector<int> &r = axis == 0 ? c.row_radices : c.col_radices;
+        for (int i = 0; i < (int)r.size() && i < capacity; ++i) radices[i] = r[i];
+        if (count) *count = (int)r.size();
+    });
+}
 size_t updc_device_bytes(updc_engine *h) { return h ? h->e->device_bytes() : 0; }
 int updc_set_stage_timing(updc_engine *h, int on) {
     return guarded([&] {
@@ -184,6 +210,51 @@ int updc_stage_update(updc_engine *h, double *sum, uint64_t *neg) {
         h->e->stage_update(&r);
         if (sum) *sum = r.signed_sum;
         if (neg) *neg = r.negative;
+    });
+}
+
+int updc_set_exposure_offsets(updc_engine *h, int k, double background, double pedestal) {
+    return guarded([&] {
+        if (!h) throw Error(1, "null handle");
+        h->e->set_exposure_offsets(k, background, pedestal);
+    });
+}
+int updc_set_psf(updc_engine *h, int k, const void *psf, int pw, int ph, int as_double) {
+    return guarded([&] {
+        if (!h || !psf) throw Error(1, "null handle or PSF");
+        h->e->set_psf(k, psf, pw, ph, as_double);
+    });
+}
+int updc_nll(updc_engine *h, double *terms) {
+    return guarded([&] {
+        if (!h || !terms) throw Error(1, "null handle or output");
+        h->e->nll(terms);
+    });
+}
+int updc_nll_partials(updc_engine *h, double *out, size_t capacity, size_t *count) {
+    return guarded([&] {
+        if (!h) throw Error(1, "null handle");
+        const std::vector<double> &p = h->e->nll_partials();
+        if (out) memcpy(out, p.data(), std::min(capacity, p.size()) * sizeof(double));
+        if (count) *count = p.size();
+    });
+}
+int updc_nll_adjoint(updc_engine *h) {
+    return guarded([&] {
+        if (!h) throw Error(1, "null handle");
+        h->e->nll_adjoint();
+    });
+}
+int updc_psf_gradient(updc_engine *h, int k, double *out) {
+    return guarded([&] {
+        if (!h || !out) throw Error(1, "null handle or output");
+        h->e->psf_gradient(k, out);
+    });
+}
+int updc_copy_plane_device(updc_engine *h, int which, int k, void *dptr, int to_engine, int as_double, void *stream) {
+    return guarded([&] {
+        if (!h || !dptr) throw Error(1, "null handle or device pointer");
+        h->e->copy_plane_device(which, k, dptr, to_engine, as_double, static_cast<cudaStream_t>(stream));
     });
 }
 
@@ -228,16 +299,72 @@ int updc_self_test(char *msg, size_t cap) {
     return rc;
 }
 
+// ---------------------------------------------------------------------------- batched fields
+int updc_batch_create(const updc_options *opt, updc_batch **out) {
+    return guarded([&] {
+        if (!out) throw Error(1, "null output handle");
+        *out = nullptr;
+        EngineOptions o = to_options(opt);
+        if (o.form < 0 || o.form > 3) throw Error(1, "unknown precision form");
+        std::unique_ptr<updc_batch> b(new updc_batch);
+        b->b = make_batch(o);
+        *out = b.release();
+    });
+}
+int updc_batch_destroy(updc_batch *b) {
+    return guarded([&] { delete b; });
+}
+int updc_batch_add_field(updc_batch *b, const char *manifest, int W, int H, int iw, int ih, int nexp, int tr) {
+    return guarded([&] {
+        if (!b || !manifest) throw Error(1, "null argument");
+        b->b->add_field(manifest, W, H, iw, ih, nexp, tr);
+        std::unique_ptr<updc_engine> v(new updc_engine);
+        v->e = &b->b->field(b->b->fields() - 1);
+        v->nexp = nexp;
+        b->views.push_back(std::move(v));
+    });
+}
+int updc_batch_setup(updc_batch *b) {
+    return guarded([&] {
+        if (!b) throw Error(1, "null handle");
+        b->b->setup();
+    });
+}
+int updc_batch_fields(updc_batch *b) { return b ? b->b->fields() : 0; }
+updc_engine *updc_batch_field(updc_batch *b, int i) {
+    if (!b || i < 0 || i >= (int)b->views.size()) return nullptr;
+    return b->views[i].get();
+}
+size_t updc_batch_units(updc_batch *b, int stage) { return b ? b->b->units(stage) : 0; }
+int updc_batch_iterate(updc_batch *b, int n, int check_each, double *seconds, double *signed_sum, uint64_t *negative,
+                       uint64_t *total_frozen) {
+    return guarded([&] {
+        if (!b) throw Error(1, "null handle");
+        std::vector<BatchRecord> recs;
+        b->b->iterate(n, check_each != 0, &recs);
+        const int nf = b->b->fields();
+        for (int i = 0; i < (int)recs.size(); ++i) {
+            if (seconds) seconds[i] = recs[i].seconds;
+            for (int f = 0; f < nf; ++f) {
+                if (signed_sum) signed_sum[(size_t)i * nf + f] = recs[i].signed_sum[f];
+                if (negative) negative[(size_t)i * nf + f] = recs[i].negative[f];
+            }
+            if (total_frozen) {
+                const size_t ne = recs[i].total_frozen.size();
+                for (size_t k = 0; k < ne; ++k) total_frozen[(size_t)i * ne + k] = recs[i].total_frozen[k];
+            }
+        }
+    });
+}
+
 // ---------------------------------------------------------------------------- UPDC_ALL
 int updc_all(const char *manifest, int width, int height, int input_width, int input_height, int exposures,
              int transpose_psf, int iterations, const char *iter_prefix, const char *weight_output,
              int fft_worker_count, int exposure_worker_count, int preprocess_worker_count, int plan_measure,
              int autotune, int retune_fft, const char *wisdom_path, int save_every) {
     return guarded([&] {
-        (void)plan_measure;
-        (void)autotune;
-        (void)retune_fft;
-        (void)wisdom_path;
+        (void)plan_measure;  // FFTW planner rigour: no counterpart (plans are timed by the autotuner)
+        (void)wisdom_path;   // FFTW wisdom file: the autotuner keeps its own cache file instead
         if (width < 1 || height < 1 || input_width < 1 || input_height < 1 || exposures < 1 || iterations < 1 ||
             fft_worker_count < 1 || exposure_worker_count < 1 || preprocess_worker_count < 1 || save_every < 0)
             throw Error(1, "invalid dimensions/exposures/iterations/workers/save_every");
@@ -250,12 +377,22 @@ int updc_all(const char *manifest, int width, int height, int input_width, int i
         if (form) o.form = atoi(form);
         o.reuse_links = persist ? 1 : 0;  // the reference rebuilds LinkMaps unless the cache is enabled
         o.verbose = 1;
+        // FFT autotune with the reference's flags and cache root (updc_core.c:130-138, 242-291)
+        o.autotune = autotune ? 1 : 0;
+        o.retune = retune_fft ? 1 : 0;
+        if (persist) {
+            const char *slash = strrchr(manifest, '/');
+            o.tune_cache_dir = slash ? std::string(manifest, slash - manifest) : std::string(".");
+        }
         std::unique_ptr<Engine> e = make_engine(o);
         e->load(manifest, width, height, input_width, input_height, exposures, transpose_psf);
         const double setup_start = wall();
         e->setup();
         const double setup_time = wall() - setup_start;
         const int FW = (int)e->scalar(2), FH = (int)e->scalar(3);
+        if (autotune)
+            printf("FFT autotune %s %dx%d (%d plans timed, modelled %.3f ms/iteration)\n",
+                   e->scalar(9) ? "persistent-cache hit:" : "selected", FW, FH, (int)e->scalar(8), e->scalar(10));
         printf("Background-aware UPDC (B200): %d exposures, input %dx%d, target %dx%d, FFT %dx%d, iterations %d\n",
                exposures, input_width, input_height, width, height, FW, FH, iterations);
         printf("WHT median normalization %.9g (%llu masked)\n", e->scalar(0), (unsigned long long)e->scalar(4));
@@ -323,7 +460,7 @@ int updc_all(const char *manifest, int width, int height, int input_width, int i
         fprintf(tf, "stage,wall_seconds\nfft_autotune,%.6f\nfft_plan,%.6f\npsf_cache,%.6f\npolygon_links,%.6f\n"
                     "persistent_mmap,%.6f\nmmap_prewarm,%.6f\ndata_cache,%.6f\nweight_scale,%.6f\ninitial_drizzle,%.6f\n"
                     "sensitivity,%.6f\n",
-                0.0, 0.0, e->setup_seconds(2), e->setup_seconds(0), 0.0, 0.0, e->setup_seconds(1), 0.0,
+                e->scalar(7), 0.0, e->setup_seconds(2), e->setup_seconds(0), 0.0, 0.0, e->setup_seconds(1), 0.0,
                 e->setup_seconds(3), e->setup_seconds(4));
         for (int i = 0; i < iterations; ++i) {
             const IterationRecord &r = recs[i];

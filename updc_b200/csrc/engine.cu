@@ -2,6 +2,9 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <functional>
+#include <map>
+#include <unistd.h>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -11,6 +14,7 @@
 #include "kernels.cuh"
 #include "linkmap.cuh"
 #include "pointwise.cuh"
+#include "nll.cuh"
 
 namespace updc {
 
@@ -90,10 +94,39 @@ bool fft_factor(int n, int rmax, std::vector<int> &radices) {
     return (int)radices.size() <= FFT_MAX_STAGES;
 }
 
-template <typename T> std::vector<cx<T>> fft_make_table(int n, int rmax, FftPlan &plan) {
-    std::vector<int> rad;
-    if (!fft_factor(n, rmax, rad)) throw Error(1, "FFT length " + std::to_string(n) + " is not 7-smooth");
+void fft_factorizations(int n, int rmax, int extra_stages, std::vector<std::vector<int>> &out) {
+    static const int order[] = {32, 28, 27, 25, 24, 21, 20, 18, 16, 15, 14, 12, 10, 9, 8, 7, 6, 5, 4, 3, 2};
+    out.clear();
+    std::vector<int> greedy;
+    if (!fft_factor(n, rmax, greedy)) return;
+    const int max_stages = (int)greedy.size() + extra_stages;
+    // depth-first over non-increasing radix sequences (the device's stage order)
+    std::vector<int> cur;
+    std::function<void(int, int)> rec = [&](int m, int first) {
+        if (m == 1) {
+            if (!cur.empty()) out.push_back(cur);
+            return;
+        }
+        if ((int)cur.size() >= max_stages) return;
+        for (int i = first; i < (int)(sizeof(order) / sizeof(order[0])); ++i) {
+            const int r = order[i];
+            if (r > rmax || m % r) continue;
+            cur.push_back(r);
+            rec(m / r, i);
+            cur.pop_back();
+        }
+    };
+    rec(n, 0);
+    if (out.empty()) out.push_back(greedy);
+}
+
+template <typename T> std::vector<cx<T>> fft_make_table(int n, const std::vector<int> &rad, FftPlan &plan) {
+    long prod = 1;
+    for (int r : rad) prod *= r;
+    if (prod != n || rad.empty() || (int)rad.size() > FFT_MAX_STAGES)
+        throw Error(1, "FFT factorization does not match length " + std::to_string(n));
     std::vector<cx<T>> tab;
+    plan = FftPlan();
     plan.n = n;
     plan.nstage = (int)rad.size();
     int ns = 1;
@@ -115,8 +148,16 @@ template <typename T> std::vector<cx<T>> fft_make_table(int n, int rmax, FftPlan
     if (tab.empty()) tab.push_back(cx<T>{1, 0});
     return tab;
 }
+
+template <typename T> std::vector<cx<T>> fft_make_table(int n, int rmax, FftPlan &plan) {
+    std::vector<int> rad;
+    if (!fft_factor(n, rmax, rad)) throw Error(1, "FFT length " + std::to_string(n) + " is not 7-smooth");
+    return fft_make_table<T>(n, rad, plan);
+}
 template std::vector<cx<float>> fft_make_table<float>(int, int, FftPlan &);
 template std::vector<cx<double>> fft_make_table<double>(int, int, FftPlan &);
+template std::vector<cx<float>> fft_make_table<float>(int, const std::vector<int> &, FftPlan &);
+template std::vector<cx<double>> fft_make_table<double>(int, const std::vector<int> &, FftPlan &);
 
 namespace {
 // Output slot of register p in the codelet of radix R (Dft<R>::out).
@@ -190,28 +231,10 @@ int fft_choose_padding(const FftPlan &plan, int nt, int cap, int batch) {
 
 namespace {
 
-// Threads per block of the spectral kernels: 512 (two blocks per SM) except
-// the FP32 adjoint column kernel, whose accumulator plane limits it to one
-// block per SM and which therefore runs 1024 threads (FP64 butterflies need
-// the 128-register budget of 512-thread blocks).
-constexpr int NT = 512;
-template <typename T> struct NtAdj {
-    static constexpr int value = sizeof(T) == 4 ? 1024 : 512;
-};
-constexpr size_t SMEM_LIMIT = 227 * 1024;
-
-// Shared-memory capacity (complex elements) of the FFT instantiations.
-template <typename T> struct Caps;
-template <> struct Caps<float> {
-    static constexpr int ROW = 5632;
-    static constexpr int COL_S = 5632;
-    static constexpr int COL_L = 11264;
-};
-template <> struct Caps<double> {
-    static constexpr int ROW = 5632;
-    static constexpr int COL_S = 5632;
-    static constexpr int COL_L = 11264;
-};
+constexpr int NT = SPEC_NT;
+template <typename T> using NtAdj = SpecNtAdj<T>;
+template <typename T> using Caps = SpecCaps<T>;
+constexpr size_t SMEM_LIMIT = SPEC_SMEM_LIMIT;
 
 template <typename T> T *dalloc(size_t n, size_t *counter) {
     T *p = nullptr;
@@ -254,11 +277,13 @@ template <typename T> class EngineImpl final : public Engine {
                                             : (opt_.form == FORM_FP32 || opt_.form == FORM_FP32_KAHAN ? 1 : 0);
     }
     ~EngineImpl() override {
+        drop_loop_graphs();
         if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
         if (graph_) cudaGraphDestroy(graph_);
         for (auto &m : links_) m.release();
         for (void *p : allocs_) cudaFree(p);
         if (staging_) cudaFree(staging_);
+        if (d_psf_grad_) cudaFree(d_psf_grad_);
         if (pinned_) cudaFreeHost(pinned_);
         for (auto e : events_) cudaEventDestroy(e);
         if (stream_) cudaStreamDestroy(stream_);
@@ -339,19 +364,16 @@ template <typename T> class EngineImpl final : public Engine {
         }
         const size_t rec_bytes = rec_stride();
         ensure_pinned((size_t)n * rec_bytes);
+        // without per-iteration checks the whole loop of n iterations is one
+        // CUDA graph (iterations, their events and record copies)
+        const bool whole = graph && !check_each && n > 1 && n <= LOOP_GRAPH_MAX;
         int done = 0;
         while (done < n) {
             const int batch = check_each ? 1 : n - done;
-            for (int i = 0; i < batch; ++i) {
-                UPDC_CUDA(cudaEventRecord(events_[2 * (done + i)], stream_));
-                if (graph) UPDC_CUDA(cudaGraphLaunch(graph_exec_, stream_));
-                else enqueue_iteration(opt_.stage_timing != 0);
-                UPDC_CUDA(cudaEventRecord(events_[2 * (done + i) + 1], stream_));
-                char *dst = (char *)pinned_ + (size_t)(done + i) * rec_bytes;
-                UPDC_CUDA(cudaMemcpyAsync(dst, d_stats_, nexp_ * sizeof(ExpStats), cudaMemcpyDeviceToHost, stream_));
-                UPDC_CUDA(cudaMemcpyAsync(dst + nexp_ * sizeof(ExpStats), d_err_, 8, cudaMemcpyDeviceToHost, stream_));
-                UPDC_CUDA(cudaMemcpyAsync(dst + nexp_ * sizeof(ExpStats) + 8, d_red_sum_, 8, cudaMemcpyDeviceToHost, stream_));
-                UPDC_CUDA(cudaMemcpyAsync(dst + nexp_ * sizeof(ExpStats) + 16, d_red_neg_, 8, cudaMemcpyDeviceToHost, stream_));
+            if (whole) {
+                UPDC_CUDA(cudaGraphLaunch(loop_graph(n), stream_));
+            } else {
+                for (int i = 0; i < batch; ++i) enqueue_recorded(done + i, graph);
             }
             UPDC_CUDA(cudaStreamSynchronize(stream_));
             for (int i = 0; i < batch; ++i) {
@@ -472,6 +494,175 @@ template <typename T> class EngineImpl final : public Engine {
             UPDC_CUDA(cudaMemcpy(&rec->negative, d_red_neg_, 8, cudaMemcpyDeviceToHost));
         }
     }
+    FieldView field_view() const override {
+        if (!setup_done_) throw Error(1, "engine is not set up");
+        FieldView v;
+        v.elem_bytes = sizeof(T);
+        v.form = opt_.form;
+        v.comp_mu = comp_mu_;
+        v.W = W_, v.H = H_, v.M = M_, v.FH = FH_, v.ldh = ldh_, v.row_b = row_b_, v.nexp = nexp_;
+        v.upd_grid = upd_grid_;
+        v.nin = nin_, v.nout = nout_;
+        v.plan_m = plan_m_, v.plan_h = plan_h_;
+        v.scale = (double)scale_factor();
+        v.max_sens = (double)max_sens_;
+        v.post = post_;
+        v.estimate = estimate_, v.den = den_, v.correction = correction_, v.blur = blur_, v.scatter = scatter_, v.wr = wr_;
+        v.rx = rx_, v.y = y_, v.rs = rs_, v.cr = cr_, v.khat = khat_;
+        bool adj = false;
+        if constexpr (sizeof(T) == 4) {
+            if (opt_.form == FORM_FP32) adj = adj_aux<AccF64>();
+            else if (opt_.form == FORM_FP32_KAHAN) adj = adj_aux<AccKahan>();
+            else adj = adj_aux<AccPlain<T>>();
+        } else {
+            adj = adj_aux<AccPlain<T>>();
+        }
+        v.needs_aux = aux_fwd_ != nullptr || adj || FH_ > Caps<T>::COL_S;
+        v.exps = d_exps_;
+        v.stats = d_stats_;
+        v.err = d_err_;
+        v.part_sum = d_part_sum_, v.part_neg = d_part_neg_, v.red_sum = d_red_sum_, v.red_neg = d_red_neg_;
+        return v;
+    }
+
+    // ------------------------------------------------------------------ differentiable model
+    void set_exposure_offsets(int k, double background, double pedestal) override {
+        if (k < 0 || k >= nexp_) throw Error(1, "exposure index out of range");
+        if (!std::isfinite(background) || !std::isfinite(pedestal) || pedestal < 0)
+            throw Error(1, "invalid background/pedestal");
+        ExposureInput &e = exps_[k];
+        e.background = background;
+        e.pedestal = pedestal;
+        e.backgroundf = (float)background;
+        e.pedestalf = (float)pedestal;
+        upload_descs();
+    }
+    void set_psf(int k, const void *psf, int pw, int phh, int as_double) override {
+        if (k < 0 || k >= nexp_) throw Error(1, "exposure index out of range");
+        const int tw = transposed_ ? phh : pw, th = transposed_ ? pw : phh;
+        if (pw < 1 || phh < 1 || W_ + tw - 1 > FW_ || H_ + th - 1 > FH_)
+            throw Error(1, "PSF larger than the FFT shape allows");
+        const size_t nu = (size_t)M_ + 1;
+        cx<T> *rp = scratch_spec(0);
+        const bool fp64_sum = opt_.form == FORM_FP32 || opt_.form == FORM_FP64;
+        if (as_double)
+            psf_spectrum_one<T, double>((const double *)psf, pw, phh, khat_ + (size_t)k * nu * FH_, rp, fp64_sum,
+                                        plan_m_, plan_h_, post_);
+        else
+            psf_spectrum_one<T, float>((const float *)psf, pw, phh, khat_ + (size_t)k * nu * FH_, rp, fp64_sum,
+                                       plan_m_, plan_h_, post_);
+        exps_[k].psf_width = pw;
+        exps_[k].psf_height = phh;
+    }
+    void nll(double *terms) override {
+        stage_forward(0);
+        const unsigned g = (unsigned)std::min<size_t>(ceil_div(nin_, 256), 148 * 4);
+        if (!d_nll_part_) d_nll_part_ = alloc<double>((size_t)g * nexp_ * NLL_TERMS);
+        k_nll<T><<<dim3(g, (unsigned)nexp_), 256, 0, stream_>>>(d_exps_, nin_, nout_, blur_, wr_, d_nll_part_);
+        UPDC_CUDA(cudaGetLastError());
+        std::vector<double> &h = nll_parts_;
+        h.assign((size_t)g * nexp_ * NLL_TERMS, 0.0);
+        UPDC_CUDA(cudaMemcpyAsync(h.data(), d_nll_part_, h.size() * 8, cudaMemcpyDeviceToHost, stream_));
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+        // block partials summed in block order with Neumaier compensation
+        for (int k = 0; k < nexp_; ++k)
+            for (int i = 0; i < NLL_TERMS; ++i) {
+                double t = 0, c = 0;
+                for (unsigned b = 0; b < g; ++b) {
+                    const double v = h[((size_t)k * g + b) * NLL_TERMS + i], u = t + v;
+                    c += std::fabs(t) >= std::fabs(v) ? (t - u) + v : (v - u) + t;
+                    t = u;
+                }
+                terms[k * NLL_TERMS + i] = t + c;
+            }
+    }
+    // Per-block partial sums of the last nll() (nexp x blocks x 4): the
+    // difference of two evaluations taken partial by partial is exact where
+    // the inputs did not change, which finite differences of single pixels need.
+    std::vector<double> nll_parts_;
+    const std::vector<double> &nll_partials() const override { return nll_parts_; }
+    void nll_adjoint() override {
+        launch_scatter(wr_, scatter_);
+        stage_correction();
+    }
+    void psf_gradient(int k, double *out) override {
+        if (k < 0 || k >= nexp_) throw Error(1, "exposure index out of range");
+        const ExposureInput &e = exps_[k];
+        const size_t nu = (size_t)M_ + 1, ns = nu * FH_;
+        cx<T> *xs = scratch_spec(0), *as = scratch_spec(1);
+        // X = FFT2(pad(x)), A = FFT2(pad(S^T r_k)), both u-major (M+1) x FH
+        launch_row_r2c_plane(estimate_, rx_, 1, 0, map_rx_);
+        launch_col_fft<false>(rx_, ldh_, H_, xs, FH_, FH_);
+        launch_row_r2c_plane(scatter_ + (size_t)k * nout_, rs_, 1, 0, map_rs_);
+        launch_col_fft<false>(rs_, ldh_, H_, as, FH_, FH_);
+        // correlation c = IFFT2(A conj(X)) / nf, kept on the PSF window
+        k_mul_conj<T><<<grid1d(ns), 256, 0, stream_>>>(as, xs, ns);
+        launch_col_fft<true>(as, FH_, FH_, xs, FH_, FH_);
+        const size_t count = (size_t)e.psf_width * e.psf_height;
+        if (!d_psf_grad_ || psf_grad_count_ < count) {
+            if (d_psf_grad_) cudaFree(d_psf_grad_);
+            d_psf_grad_ = dalloc<double>(count, nullptr);
+            psf_grad_count_ = count;
+        }
+        UPDC_CUDA(cudaMemsetAsync(d_psf_grad_, 0, count * 8, stream_));
+        const int fwid = transposed_ ? e.psf_height : e.psf_width, fhei = transposed_ ? e.psf_width : e.psf_height;
+        const PsfWindowStore<T> epi{d_psf_grad_, e.psf_width, fwid, fhei, FW_, FH_, transposed_};
+        const int B = row_b_;
+        const size_t rsm = row_buf_bytes(B, M_, sizeof(cx<T>), plan_m_.pad_shift);
+        set_smem(k_row_c2r<T, NT, Caps<T>::ROW, PsfWindowStore<T>, false>, rsm);
+        dim3 grid((unsigned)ceil_div(FH_, B), 1);
+        k_row_c2r<T, NT, Caps<T>::ROW, PsfWindowStore<T>, false><<<grid, NT, rsm, stream_>>>(
+            plan_m_, post_, SpecRef{xs, FH_, 0}, no_map_, FH_, FW_, B, FastDiv((uint32_t)B),
+            (T)(1.0 / ((double)FW_ * (double)FH_)), epi, d_err_);
+        UPDC_CUDA(cudaGetLastError());
+        UPDC_CUDA(cudaMemcpyAsync(out, d_psf_grad_, count * 8, cudaMemcpyDeviceToHost, stream_));
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+    }
+    void copy_plane_device(int which, int k, void *dptr, int to_engine, int as_double, cudaStream_t stream) override {
+        if (which == PLANE_FROZEN) throw Error(1, "device copies cover the floating-point planes");
+        size_t n;
+        void *plane = const_cast<void *>(plane_ptr(which, k, &n));
+        // order the engine's stream after the caller's
+        cudaEvent_t ev;
+        UPDC_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        UPDC_CUDA(cudaEventRecord(ev, stream));
+        UPDC_CUDA(cudaStreamWaitEvent(stream_, ev, 0));
+        cudaEventDestroy(ev);
+        const bool same = (as_double != 0) == (sizeof(T) == 8);
+        if (to_engine) {
+            if (same) UPDC_CUDA(cudaMemcpyAsync(plane, dptr, n * sizeof(T), cudaMemcpyDeviceToDevice, stream_));
+            else if (as_double) k_convert<double, T><<<grid1d(n), 256, 0, stream_>>>((const double *)dptr, (T *)plane, n);
+            else k_convert<float, T><<<grid1d(n), 256, 0, stream_>>>((const float *)dptr, (T *)plane, n);
+        } else {
+            if (same) UPDC_CUDA(cudaMemcpyAsync(dptr, plane, n * sizeof(T), cudaMemcpyDeviceToDevice, stream_));
+            else if (as_double) k_convert<T, double><<<grid1d(n), 256, 0, stream_>>>((const T *)plane, (double *)dptr, n);
+            else k_convert<T, float><<<grid1d(n), 256, 0, stream_>>>((const T *)plane, (float *)dptr, n);
+        }
+        UPDC_CUDA(cudaGetLastError());
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+    }
+    double *d_nll_part_ = nullptr, *d_psf_grad_ = nullptr;
+    size_t psf_grad_count_ = 0;
+    cx<T> *scratch_spec_[2] = {nullptr, nullptr};
+    // (M+1) x FH complex scratch planes of the differentiable-model paths
+    cx<T> *scratch_spec(int i) {
+        if (!scratch_spec_[i]) scratch_spec_[i] = alloc<cx<T>>(((size_t)M_ + 1) * FH_);
+        return scratch_spec_[i];
+    }
+    // column transforms of M+1 columns: `in` has `rows_in` rows at pitch ldi
+    template <bool INV> void launch_col_fft(const cx<T> *in, int ldi, int rows_in, cx<T> *out, int ldo, int rows_out) {
+        const size_t nu = (size_t)M_ + 1;
+        const size_t cs = fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift);
+        if (FH_ <= Caps<T>::COL_S) {
+            set_smem(k_col_fft<T, NT, Caps<T>::COL_S, INV>, cs);
+            k_col_fft<T, NT, Caps<T>::COL_S, INV><<<(unsigned)nu, NT, cs, stream_>>>(plan_h_, in, ldi, rows_in, out, ldo, rows_out);
+        } else {
+            set_smem(k_col_fft<T, NT, Caps<T>::COL_L, INV>, cs);
+            k_col_fft<T, NT, Caps<T>::COL_L, INV><<<(unsigned)nu, NT, cs, stream_>>>(plan_h_, in, ldi, rows_in, out, ldo, rows_out);
+        }
+        UPDC_CUDA(cudaGetLastError());
+    }
+
     void decode_links(int k, uint32_t *host_targets) override {
         const DevLinkMap &m = links_.at(k);
         uint32_t *d = dalloc<uint32_t>(m.nlinks, nullptr);
@@ -491,6 +682,10 @@ template <typename T> class EngineImpl final : public Engine {
             case 4: return (double)masked_;
             case 5: return sizeof(T) * 8;
             case 6: return comp_mu_;
+            case 7: return choice_.seconds;
+            case 8: return choice_.candidates;
+            case 9: return choice_.cache_hit ? 1 : 0;
+            case 10: return choice_.predicted_ms;
             default: return 0;
         }
     }
@@ -541,12 +736,275 @@ template <typename T> class EngineImpl final : public Engine {
     size_t rec_stride() const { return align16(nexp_ * sizeof(ExpStats) + 24); }
     void ensure_pinned(size_t bytes) {
         if (bytes <= pinned_bytes_) return;
+        drop_loop_graphs();  // they copy into the old buffer
         if (pinned_) cudaFreeHost(pinned_);
         UPDC_CUDA(cudaMallocHost(&pinned_, bytes));
         pinned_bytes_ = bytes;
     }
 
     bool acc_fp64() const { return opt_.form == FORM_FP32 && sizeof(T) == 4; }
+
+    // ------------------------------------------------------------------ FFT shape and autotuner
+    // The padded FFT shape follows select_fft_shape (updc_core.c:242-291):
+    // without autotuning the smallest 7-smooth sizes >= W + pw - 1 and
+    // H + ph - 1 (even width here: the row transform is a half-length complex
+    // FFT).  With autotuning the candidate shapes are the reference's (five
+    // fast sizes per axis, the diagonal pairs and four off-diagonal ones), and
+    // for each axis length every radix split within one stage of the fewest is
+    // timed with the engine's own row and column kernels on scratch planes;
+    // the shape with the smallest modelled spectral time per iteration wins.
+    // The choice is cached like the reference's fft_autotune_v1 files
+    // (updc_core.c:195-230), keyed by the device instead of FFTW's version.
+    FftChoice choice_;
+    const FftChoice &fft_choice() const override { return choice_; }
+
+    static std::vector<int> fast_candidates(int minimum, bool even, int count, int cap) {
+        std::vector<int> out;
+        for (int v = minimum; (int)out.size() < count; ++v) {
+            v = next_smooth(v, even);
+            if (v > cap) break;
+            out.push_back(v);
+        }
+        return out;
+    }
+
+    std::string tune_cache_path(int min_w, int min_h) const {
+        if (opt_.tune_cache_dir.empty()) return "";
+        char name[160];
+        snprintf(name, sizeof(name), "fft_autotune_b200_v1_%s_%dx%d_h%d_n%d.txt", sizeof(T) == 4 ? "f32" : "f64",
+                 min_w, min_h, H_, nexp_);
+        return opt_.tune_cache_dir + "/" + name;
+    }
+    std::string device_signature() const {
+        cudaDeviceProp p;
+        UPDC_CUDA(cudaGetDeviceProperties(&p, opt_.device));
+        int rt = 0;
+        cudaRuntimeGetVersion(&rt);
+        char sig[400];
+        snprintf(sig, sizeof(sig), "%s|sm%d%d|%d SMs|cudart %d|updc_b200 tuner 1", p.name, p.major, p.minor,
+                 p.multiProcessorCount, rt);
+        return sig;
+    }
+    static std::string radix_text(const std::vector<int> &r) {
+        std::string t;
+        for (size_t i = 0; i < r.size(); ++i) t += (i ? "," : "") + std::to_string(r[i]);
+        return t;
+    }
+    static std::vector<int> radix_parse(const char *t) {
+        std::vector<int> r;
+        for (const char *c = t; *c;) {
+            char *e = nullptr;
+            const long v = strtol(c, &e, 10);
+            if (e == c) break;
+            r.push_back((int)v);
+            c = *e == ',' ? e + 1 : e;
+        }
+        return r;
+    }
+    bool load_tune_cache(const std::string &path, int min_w, int min_h, FftChoice &c) const {
+        if (path.empty() || opt_.retune) return false;
+        FILE *f = fopen(path.c_str(), "r");
+        if (!f) return false;
+        char sig[400] = {}, rr[200] = {}, cr[200] = {};
+        int mw = 0, mh = 0, w = 0, h = 0;
+        double ms = 0;
+        const bool ok = fscanf(f, "signature=%399[^\n]\nmin_width=%d\nmin_height=%d\nwidth=%d\nheight=%d\n"
+                                  "row_radices=%199[^\n]\ncol_radices=%199[^\n]\npredicted_ms=%lf\n",
+                               sig, &mw, &mh, &w, &h, rr, cr, &ms) == 8;
+        fclose(f);
+        if (!ok || device_signature() != sig || mw != min_w || mh != min_h || w < min_w || h < min_h || (w & 1))
+            return false;
+        c.width = w;
+        c.height = h;
+        c.row_radices = radix_parse(rr);
+        c.col_radices = radix_parse(cr);
+        c.predicted_ms = ms;
+        long pr = 1, pc = 1;
+        for (int r : c.row_radices) pr *= r;
+        for (int r : c.col_radices) pc *= r;
+        return pr == w / 2 && pc == h;
+    }
+    void save_tune_cache(const std::string &path, int min_w, int min_h, const FftChoice &c) const {
+        if (path.empty()) return;
+        const std::string tmp = path + ".tmp." + std::to_string((long)getpid());
+        FILE *f = fopen(tmp.c_str(), "w");
+        if (!f) return;
+        fprintf(f, "signature=%s\nmin_width=%d\nmin_height=%d\nwidth=%d\nheight=%d\nrow_radices=%s\ncol_radices=%s\n"
+                   "predicted_ms=%.6f\n",
+                device_signature().c_str(), min_w, min_h, c.width, c.height, radix_text(c.row_radices).c_str(),
+                radix_text(c.col_radices).c_str(), c.predicted_ms);
+        if (fclose(f) || rename(tmp.c_str(), path.c_str())) unlink(tmp.c_str());
+    }
+
+    // Device time (ms, best of 3 after one warm-up) of a launch sequence.
+    template <class F> float time_launch(F &&launch) {
+        cudaEvent_t a, b;
+        UPDC_CUDA(cudaEventCreate(&a));
+        UPDC_CUDA(cudaEventCreate(&b));
+        float best = 1e30f;
+        launch();
+        for (int r = 0; r < 3; ++r) {
+            UPDC_CUDA(cudaEventRecord(a, stream_));
+            launch();
+            UPDC_CUDA(cudaEventRecord(b, stream_));
+            UPDC_CUDA(cudaEventSynchronize(b));
+            float ms = 0;
+            UPDC_CUDA(cudaEventElapsedTime(&ms, a, b));
+            best = std::min(best, ms);
+        }
+        UPDC_CUDA(cudaGetLastError());
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        return best;
+    }
+
+    // Candidate splits of an axis length (at most one stage more than the
+    // fewest), fewest stages first, at most 20.
+    static std::vector<std::vector<int>> split_candidates(int n) {
+        std::vector<std::vector<int>> all;
+        fft_factorizations(n, FFT_RMAX, 1, all);
+        std::stable_sort(all.begin(), all.end(), [](const std::vector<int> &a, const std::vector<int> &b) {
+            return a.size() < b.size();
+        });
+        if (all.size() > 20) all.resize(20);
+        return all;
+    }
+
+    // Times the row transform (R2C of H rows of a W-wide plane into an M-point
+    // spectrum) for every split of M; returns the best split and its time.
+    std::pair<std::vector<int>, float> tune_row(int M, const T *plane, cx<T> *spec, int *timed) {
+        std::pair<std::vector<int>, float> best{{}, 1e30f};
+        const int nu = M + 1, fw = 2 * M;
+        int B = std::max(1, std::min(Caps<T>::ROW / M, H_));
+        if (sizeof(T) == 4 && B >= 2) B &= ~1;
+        std::vector<cx<T>> post(nu);
+        const double two_pi = 6.283185307179586476925286766559;
+        for (int u = 0; u <= M; ++u) post[u] = cx<T>{(T)std::cos(-two_pi * u / fw), (T)std::sin(-two_pi * u / fw)};
+        cx<T> *dpost = dalloc<cx<T>>(nu, nullptr);
+        UPDC_CUDA(cudaMemcpy(dpost, post.data(), nu * sizeof(cx<T>), cudaMemcpyHostToDevice));
+        for (const auto &rad : split_candidates(M)) {
+            FftPlan plan;
+            auto tab = fft_make_table<T>(M, rad, plan);
+            plan.pad_shift = fft_choose_padding(plan, NT, Caps<T>::ROW, std::max(1, std::min(2, Caps<T>::ROW / M)));
+            const size_t smem = row_buf_bytes(B, M, sizeof(cx<T>), plan.pad_shift);
+            if (smem > SMEM_LIMIT) continue;
+            cx<T> *dtab = dalloc<cx<T>>(tab.size(), nullptr);
+            UPDC_CUDA(cudaMemcpy(dtab, tab.data(), tab.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
+            plan.tw = dtab;
+            set_smem(k_row_r2c<T, NT, Caps<T>::ROW, PlaneLoader<T>, false>, smem);
+            const PlaneLoader<T> ld{plane, W_, 0};
+            dim3 grid((unsigned)ceil_div(H_, B), 1);
+            const float ms = time_launch([&] {
+                k_row_r2c<T, NT, Caps<T>::ROW, PlaneLoader<T>, false><<<grid, NT, smem, stream_>>>(
+                    plan, dpost, ld, W_, H_, B, FastDiv((uint32_t)B), SpecRef{spec, H_, 0}, no_map_);
+            });
+            ++*timed;
+            cudaFree(dtab);
+            if (ms < best.second) best = {rad, ms};
+        }
+        cudaFree(dpost);
+        return best;
+    }
+
+    // Times the column transform (nc columns of length FH, H input rows) for
+    // every split of FH; returns the best split and its time per column.
+    std::pair<std::vector<int>, float> tune_col(int FH, int nc, const cx<T> *in, cx<T> *out, int *timed) {
+        std::pair<std::vector<int>, float> best{{}, 1e30f};
+        for (const auto &rad : split_candidates(FH)) {
+            FftPlan plan;
+            auto tab = fft_make_table<T>(FH, rad, plan);
+            plan.pad_shift = fft_choose_padding(plan, NT, Caps<T>::COL_S, 1);
+            const size_t smem = fft_buf_bytes(FH, sizeof(cx<T>), plan.pad_shift);
+            if (smem > SMEM_LIMIT) continue;
+            cx<T> *dtab = dalloc<cx<T>>(tab.size(), nullptr);
+            UPDC_CUDA(cudaMemcpy(dtab, tab.data(), tab.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
+            plan.tw = dtab;
+            float ms;
+            if (FH <= Caps<T>::COL_S) {
+                set_smem(k_col_fft<T, NT, Caps<T>::COL_S, false>, smem);
+                ms = time_launch([&] {
+                    k_col_fft<T, NT, Caps<T>::COL_S, false><<<(unsigned)nc, NT, smem, stream_>>>(plan, in, H_, H_, out, FH, FH);
+                });
+            } else {
+                set_smem(k_col_fft<T, NT, Caps<T>::COL_L, false>, smem);
+                ms = time_launch([&] {
+                    k_col_fft<T, NT, Caps<T>::COL_L, false><<<(unsigned)nc, NT, smem, stream_>>>(plan, in, H_, H_, out, FH, FH);
+                });
+            }
+            ++*timed;
+            cudaFree(dtab);
+            if (ms / nc < best.second) best = {rad, ms / nc};
+        }
+        return best;
+    }
+
+    void autotune_shape(int min_w, int min_h, FftChoice &c) {
+        const double t0 = now_s();
+        std::vector<int> wc = opt_.fft_width ? std::vector<int>{opt_.fft_width}
+                                             : fast_candidates(min_w, true, 5, 2 * Caps<T>::ROW);
+        std::vector<int> hc = opt_.fft_height ? std::vector<int>{opt_.fft_height}
+                                              : fast_candidates(min_h, false, 5, Caps<T>::COL_L);
+        if (wc.empty() || hc.empty()) throw Error(1, "no FFT shape within the transform capacity");
+        std::vector<std::pair<int, int>> shapes;
+        auto add = [&](size_t i, size_t j) {
+            if (i >= wc.size() || j >= hc.size()) return;
+            for (auto &s : shapes)
+                if (s.first == wc[i] && s.second == hc[j]) return;
+            shapes.push_back({wc[i], hc[j]});
+        };
+        for (size_t i = 0; i < std::min(wc.size(), hc.size()); ++i) add(i, i);
+        add(2, 0), add(0, 2), add(4, 0), add(0, 4);
+        if (wc.size() == 1 || hc.size() == 1)
+            for (size_t i = 0; i < wc.size(); ++i)
+                for (size_t j = 0; j < hc.size(); ++j) add(i, j);
+        // scratch: one target plane, its widest row spectrum, NC columns out
+        const int NC = 148 * 8;
+        const int mmax = *std::max_element(wc.begin(), wc.end()) / 2;
+        const int hmax = *std::max_element(hc.begin(), hc.end());
+        T *plane = dalloc<T>(nout_, nullptr);
+        UPDC_CUDA(cudaMemset(plane, 0, nout_ * sizeof(T)));
+        cx<T> *spec = dalloc<cx<T>>((size_t)(mmax + 1) * H_, nullptr);
+        cx<T> *cols = dalloc<cx<T>>((size_t)NC * hmax, nullptr);
+        UPDC_CUDA(cudaMemset(spec, 0, (size_t)(mmax + 1) * H_ * sizeof(cx<T>)));
+        std::map<int, std::pair<std::vector<int>, float>> rows, colsb;
+        int timed = 0;
+        try {
+            for (auto &s : shapes) {
+                if (!rows.count(s.first / 2)) rows[s.first / 2] = tune_row(s.first / 2, plane, spec, &timed);
+                if (!colsb.count(s.second))
+                    colsb[s.second] = tune_col(s.second, std::min(NC, mmax + 1), spec, cols, &timed);
+            }
+        } catch (...) {
+            cudaFree(plane), cudaFree(spec), cudaFree(cols);
+            throw;
+        }
+        cudaFree(plane), cudaFree(spec), cudaFree(cols);
+        // per iteration: 2N+2 row passes and 2N+2 column transforms over
+        // M+1 columns, plus 2N reads of a PSF spectrum (HBM, ~6.5 TB/s)
+        double best = 1e300;
+        for (auto &s : shapes) {
+            const auto &r = rows[s.first / 2], &q = colsb[s.second];
+            if (r.first.empty() || q.first.empty()) continue;
+            const int nu = s.first / 2 + 1;
+            const double otf_ms = 2.0 * nexp_ * (double)nu * s.second * sizeof(cx<T>) / 6.5e12 * 1e3;
+            const double ms = (2.0 * nexp_ + 2.0) * (r.second + (double)q.second * nu) + otf_ms;
+            if (opt_.verbose)
+                printf("FFT candidate %dx%d rows [%s] %.4f ms, columns [%s] %.4f ms, modelled %.3f ms/iteration\n",
+                       s.first, s.second, radix_text(r.first).c_str(), r.second, radix_text(q.first).c_str(),
+                       q.second * nu, ms);
+            if (ms < best) {
+                best = ms;
+                c.width = s.first;
+                c.height = s.second;
+                c.row_radices = r.first;
+                c.col_radices = q.first;
+            }
+        }
+        if (c.row_radices.empty()) throw Error(1, "FFT autotune found no usable plan");
+        c.predicted_ms = best;
+        c.candidates = timed;
+        c.seconds = now_s() - t0;
+    }
 
     void choose_fft_shape() {
         int mpw = 0, mph = 0;
@@ -556,15 +1014,38 @@ template <typename T> class EngineImpl final : public Engine {
         }
         const int pad_w = transposed_ ? mph : mpw, pad_h = transposed_ ? mpw : mph;
         const int min_w = W_ + pad_w - 1, min_h = H_ + pad_h - 1;
-        FW_ = opt_.fft_width ? opt_.fft_width : next_smooth(min_w, true);
-        FH_ = opt_.fft_height ? opt_.fft_height : next_smooth(min_h, false);
-        if (FW_ < min_w || FH_ < min_h || (FW_ & 1)) throw Error(1, "FFT shape below the linear-convolution minimum or odd width");
+        if ((opt_.fft_width && (opt_.fft_width < min_w || (opt_.fft_width & 1))) || (opt_.fft_height && opt_.fft_height < min_h))
+            throw Error(1, "FFT shape below the linear-convolution minimum or odd width");
+        FftChoice c;
+        if (opt_.autotune) {
+            const std::string cache = tune_cache_path(min_w, min_h);
+            const double t0 = now_s();
+            if (load_tune_cache(cache, min_w, min_h, c) && (!opt_.fft_width || c.width == opt_.fft_width) &&
+                (!opt_.fft_height || c.height == opt_.fft_height)) {
+                c.cache_hit = true;
+                c.seconds = now_s() - t0;
+            } else {
+                c = FftChoice();
+                autotune_shape(min_w, min_h, c);
+                save_tune_cache(cache, min_w, min_h, c);
+            }
+        } else {
+            c.width = opt_.fft_width ? opt_.fft_width : next_smooth(min_w, true);
+            c.height = opt_.fft_height ? opt_.fft_height : next_smooth(min_h, false);
+        }
+        FW_ = c.width;
+        FH_ = c.height;
         M_ = FW_ / 2;
         if (M_ > Caps<T>::ROW) throw Error(1, "FFT width exceeds the row-transform capacity");
         if (FH_ > Caps<T>::COL_L) throw Error(1, "FFT height exceeds the column-transform capacity");
+        if (c.row_radices.empty() && !fft_factor(M_, FFT_RMAX, c.row_radices))
+            throw Error(1, "FFT length " + std::to_string(M_) + " is not 7-smooth");
+        if (c.col_radices.empty() && !fft_factor(FH_, FFT_RMAX, c.col_radices))
+            throw Error(1, "FFT length " + std::to_string(FH_) + " is not 7-smooth");
+        choice_ = c;
         // twiddle tables
-        auto tm = fft_make_table<T>(M_, FFT_RMAX, plan_m_);
-        auto th = fft_make_table<T>(FH_, FFT_RMAX, plan_h_);
+        auto tm = fft_make_table<T>(M_, c.row_radices, plan_m_);
+        auto th = fft_make_table<T>(FH_, c.col_radices, plan_h_);
         plan_m_.pad_shift = fft_choose_padding(plan_m_, NT, Caps<T>::ROW, std::max(1, std::min(2, Caps<T>::ROW / M_)));
         plan_h_.pad_shift = fft_choose_padding(plan_h_, NT, Caps<T>::COL_S, 1);
         cx<T> *dm = alloc<cx<T>>(tm.size()), *dh = alloc<cx<T>>(th.size());
@@ -804,6 +1285,56 @@ template <typename T> class EngineImpl final : public Engine {
         }
     }
 
+    // One iteration with its events and the copies of its record into
+    // pinned slot i (stats, error key, signed sum, negative count).  Inside a
+    // capture the events become external event-record nodes, so they keep
+    // their timestamps when the graph runs.
+    void enqueue_recorded(int i, bool graph, bool capturing = false) {
+        const size_t rec_bytes = rec_stride();
+        const unsigned flags = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+        UPDC_CUDA(cudaEventRecordWithFlags(events_[2 * i], stream_, flags));
+        if (graph) UPDC_CUDA(cudaGraphLaunch(graph_exec_, stream_));
+        else enqueue_iteration(opt_.stage_timing != 0);
+        UPDC_CUDA(cudaEventRecordWithFlags(events_[2 * i + 1], stream_, flags));
+        char *dst = (char *)pinned_ + (size_t)i * rec_bytes;
+        UPDC_CUDA(cudaMemcpyAsync(dst, d_stats_, nexp_ * sizeof(ExpStats), cudaMemcpyDeviceToHost, stream_));
+        UPDC_CUDA(cudaMemcpyAsync(dst + nexp_ * sizeof(ExpStats), d_err_, 8, cudaMemcpyDeviceToHost, stream_));
+        UPDC_CUDA(cudaMemcpyAsync(dst + nexp_ * sizeof(ExpStats) + 8, d_red_sum_, 8, cudaMemcpyDeviceToHost, stream_));
+        UPDC_CUDA(cudaMemcpyAsync(dst + nexp_ * sizeof(ExpStats) + 16, d_red_neg_, 8, cudaMemcpyDeviceToHost, stream_));
+    }
+
+    // Graph of n whole iterations (cached per n; rebuilt if the pinned
+    // record buffer moves).
+    static constexpr int LOOP_GRAPH_MAX = 256;
+    std::map<int, cudaGraphExec_t> loop_graphs_;
+    void drop_loop_graphs() {
+        for (auto &g : loop_graphs_) cudaGraphExecDestroy(g.second);
+        loop_graphs_.clear();
+    }
+    cudaGraphExec_t loop_graph(int n) {
+        auto it = loop_graphs_.find(n);
+        if (it != loop_graphs_.end()) return it->second;
+        if (loop_graphs_.size() >= 8) drop_loop_graphs();
+        reset_iteration_state();
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+        cudaGraph_t g = nullptr;
+        UPDC_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        try {
+            for (int i = 0; i < n; ++i) enqueue_recorded(i, false, true);
+        } catch (...) {
+            cudaStreamEndCapture(stream_, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        UPDC_CUDA(cudaStreamEndCapture(stream_, &g));
+        cudaGraphExec_t ex = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+        cudaGraphDestroy(g);
+        UPDC_CUDA(e);
+        loop_graphs_[n] = ex;
+        return ex;
+    }
+
     void build_graph() {
         // the stats-initialiser buffer must exist before capture
         reset_iteration_state();
@@ -954,23 +1485,44 @@ template <typename T> class EngineImpl final : public Engine {
 
     // PSF spectra K_k (u-major, (M+1) x FH) of precision U into dst.
     template <typename U>
-    void psf_spectra(cx<U> *dst, bool fp64_sum, const FftPlan &pm, const FftPlan &ph,
-                     const cx<U> *post) {
+    void psf_spectra(cx<U> *dst, bool fp64_sum, const FftPlan &pm, const FftPlan &ph, const cx<U> *post) {
         const size_t nu = (size_t)M_ + 1;
         cx<U> *rp = dalloc<cx<U>>(nu * FH_, nullptr);
-        for (int k = 0; k < nexp_; ++k) {
-            const ExposureInput &e = exps_[k];
-            const size_t count = (size_t)e.psf_width * e.psf_height;
-            std::vector<float> hp(count);
-            if (!read_f32_exact(e.psf, hp.data(), count)) { cudaFree(rp); throw Error(1, "cannot read PSF raw: " + e.psf); }
-            float *dp = dalloc<float>(count, nullptr);
-            UPDC_CUDA(cudaMemcpy(dp, hp.data(), count * 4, cudaMemcpyHostToDevice));
+        try {
+            for (int k = 0; k < nexp_; ++k) {
+                const ExposureInput &e = exps_[k];
+                const size_t count = (size_t)e.psf_width * e.psf_height;
+                std::vector<float> hp(count);
+                if (!read_f32_exact(e.psf, hp.data(), count)) throw Error(1, "cannot read PSF raw: " + e.psf);
+                psf_spectrum_one<U, float>(hp.data(), e.psf_width, e.psf_height, dst + (size_t)k * nu * FH_, rp,
+                                           fp64_sum, pm, ph, post);
+            }
+        } catch (...) {
+            cudaFree(rp);
+            throw;
+        }
+        cudaFree(rp);
+    }
+
+    // One PSF (host array, manifest layout) to its spectrum `out`: sum (FP64,
+    // or the reference's Neumaier FP32), 1/sum, centre wrap, R2C
+    // (prepare_psf_with_buffers, updc_core.c:777-843).  `rp` is an
+    // (M+1) x FH scratch.  An FP64 PSF (differentiable model) is summed in FP64.
+    template <typename U, typename P>
+    void psf_spectrum_one(const P *hp, int pw, int phh, cx<U> *out, cx<U> *rp, bool fp64_sum, const FftPlan &pm,
+                          const FftPlan &ph, const cx<U> *post) {
+        const size_t nu = (size_t)M_ + 1;
+        const size_t count = (size_t)pw * phh;
+        if (sizeof(P) == 8) fp64_sum = true;
+        P *dp = dalloc<P>(count, nullptr);
+        try {
+            UPDC_CUDA(cudaMemcpy(dp, hp, count * sizeof(P), cudaMemcpyHostToDevice));
             UPDC_CUDA(cudaMemset(d_err_, 0xFF, 8));
             double sum = 0;
             if (fp64_sum) {
                 const int g = 148;
                 double *part = dalloc<double>(g, nullptr);
-                k_psf_sum_f64<<<g, 256, 0, stream_>>>(dp, count, part, d_err_);
+                k_psf_sum_f64<P><<<g, 256, 0, stream_>>>(dp, count, part, d_err_);
                 std::vector<double> hpart(g);
                 UPDC_CUDA(cudaMemcpyAsync(hpart.data(), part, g * 8, cudaMemcpyDeviceToHost, stream_));
                 UPDC_CUDA(cudaStreamSynchronize(stream_));
@@ -978,7 +1530,7 @@ template <typename T> class EngineImpl final : public Engine {
                 cudaFree(part);
             } else {
                 float *ds = dalloc<float>(1, nullptr);
-                k_psf_sum_neumaier<<<1, 1, 0, stream_>>>(dp, count, ds, d_err_);
+                k_psf_sum_neumaier<<<1, 1, 0, stream_>>>((const float *)dp, count, ds, d_err_);
                 float hs = 0;
                 UPDC_CUDA(cudaMemcpyAsync(&hs, ds, 4, cudaMemcpyDeviceToHost, stream_));
                 UPDC_CUDA(cudaStreamSynchronize(stream_));
@@ -986,20 +1538,18 @@ template <typename T> class EngineImpl final : public Engine {
                 cudaFree(ds);
             }
             check_error();
-            if (!(sum > 0) || !std::isfinite(sum)) { cudaFree(dp); cudaFree(rp); throw Error(1, "PSF sum is zero/non-finite"); }
+            if (!(sum > 0) || !std::isfinite(sum)) throw Error(1, "PSF sum is zero/non-finite");
             U inv;
             if (fp64_sum) inv = (U)(1.0 / sum);
             else inv = (U)(1.0f / (float)sum);
-            PsfLoader<U> ld{dp, e.psf_width, transposed_ ? e.psf_height : e.psf_width,
-                            transposed_ ? e.psf_width : e.psf_height, FW_, FH_, transposed_, inv};
+            PsfLoader<U, P> ld{dp, pw, transposed_ ? phh : pw, transposed_ ? pw : phh, FW_, FH_, transposed_, inv};
             const int B = Caps<U>::ROW / M_;
             const size_t rsm = row_buf_bytes(B, M_, sizeof(cx<U>), pm.pad_shift);
-            set_smem(k_row_r2c<U, NT, Caps<U>::ROW, PsfLoader<U>, false>, rsm);
+            set_smem(k_row_r2c<U, NT, Caps<U>::ROW, PsfLoader<U, P>, false>, rsm);
             dim3 grid((unsigned)ceil_div(FH_, B), 1);
-            k_row_r2c<U, NT, Caps<U>::ROW, PsfLoader<U>, false><<<grid, NT, rsm, stream_>>>(
+            k_row_r2c<U, NT, Caps<U>::ROW, PsfLoader<U, P>, false><<<grid, NT, rsm, stream_>>>(
                 pm, post, ld, FW_, FH_, B, FastDiv((uint32_t)B), SpecRef{rp, FH_, 0}, no_map_);
             const size_t cs = fft_buf_bytes(FH_, sizeof(cx<U>), ph.pad_shift);
-            cx<U> *out = dst + (size_t)k * nu * FH_;
             if (FH_ <= Caps<U>::COL_S) {
                 set_smem(k_col_fft<U, NT, Caps<U>::COL_S, false>, cs);
                 k_col_fft<U, NT, Caps<U>::COL_S, false><<<(unsigned)nu, NT, cs, stream_>>>(ph, rp, FH_, FH_, out, FH_, FH_);
@@ -1009,9 +1559,11 @@ template <typename T> class EngineImpl final : public Engine {
             }
             UPDC_CUDA(cudaGetLastError());
             UPDC_CUDA(cudaStreamSynchronize(stream_));
+        } catch (...) {
             cudaFree(dp);
+            throw;
         }
-        cudaFree(rp);
+        cudaFree(dp);
     }
 
     void prepare_psf_spectra() {

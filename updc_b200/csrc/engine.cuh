@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "fft.cuh"
 
 namespace updc {
 
@@ -22,6 +23,19 @@ struct EngineOptions {
     int fft_width = 0;        // 0: smallest even 7-smooth width >= W + pw - 1
     int fft_height = 0;       // 0: smallest 7-smooth height >= H + ph - 1
     int stage_timing = 0;     // time each stage with events (no graph)
+    int autotune = 0;         // time candidate FFT shapes and radix splits on the device
+    int retune = 0;           // ignore a cached autotune result
+    std::string tune_cache_dir;  // directory of the autotune cache ("" = no cache)
+};
+
+// Outcome of the FFT autotuner (or of the fixed choice without it).
+struct FftChoice {
+    int width = 0, height = 0;
+    std::vector<int> row_radices, col_radices;
+    double predicted_ms = 0;  // modelled spectral time per iteration
+    int candidates = 0;       // plans timed (0: fixed choice or cache hit)
+    bool cache_hit = false;
+    double seconds = 0;       // wall time of the tuning
 };
 
 struct ExposureInput {
@@ -75,9 +89,74 @@ class Engine {
     virtual double setup_seconds(int stage) const = 0;
     // Per-stage event timing on the next iterations (eager launches, no graph).
     virtual void set_stage_timing(int on) = 0;
+    // FFT shape and radix splits in use, and how they were chosen.
+    virtual const FftChoice &fft_choice() const = 0;
+
+    // Differentiable model (nll.cuh).  Per-exposure background and pedestal,
+    // and a replacement PSF (FP32 or FP64 host array in the manifest's
+    // layout, no larger than the PSF the FFT shape was chosen for).
+    virtual void set_exposure_offsets(int k, double background, double pedestal) = 0;
+    virtual void set_psf(int k, const void *psf, int psf_width, int psf_height, int as_double) = 0;
+    // Forward model of the current estimate, then the NLL terms per exposure
+    // (nexp x 4: sum W(mu - y log mu), sum r, sum W log mu, pixels left out)
+    // and r = W (1 - y/mu) in the WR planes.
+    virtual void nll(double *terms) = 0;
+    // Per-block FP64 partial sums behind the last nll() (nexp x blocks x 4).
+    virtual const std::vector<double> &nll_partials() const = 0;
+    // CORRECTION <- sum_k H_k^T r_k = dL/dx (after nll).
+    virtual void nll_adjoint() = 0;
+    // dL/dpsi_k for the normalised PSF of exposure k, in the PSF's own layout
+    // (after nll_adjoint); psf_width x psf_height doubles.
+    virtual void psf_gradient(int k, double *out) = 0;
+    // Plane <-> caller device memory (to_engine = 1 writes the plane), on the
+    // engine's stream after `stream` (0: legacy default) has reached this call.
+    virtual void copy_plane_device(int which, int k, void *dptr, int to_engine, int as_double, cudaStream_t stream) = 0;
+    // Device-side view of the set-up field for the batched launches (batch.cu).
+    virtual struct FieldView field_view() const = 0;
+};
+
+// Everything the batched launches need of one set-up field: sizes, plans
+// and the device addresses of its planes, spectra and diagnostics (typed by
+// the engine's precision, 4 or 8 bytes).
+struct FieldView {
+    int elem_bytes = 4, form = 0, comp_mu = 0;
+    int W = 0, H = 0, M = 0, FH = 0, ldh = 0, row_b = 0, nexp = 0, upd_grid = 0;
+    size_t nin = 0, nout = 0;
+    FftPlan plan_m, plan_h;
+    double scale = 0, max_sens = 0;
+    const void *post = nullptr;
+    void *estimate = nullptr, *den = nullptr, *correction = nullptr, *blur = nullptr, *scatter = nullptr, *wr = nullptr;
+    void *rx = nullptr, *y = nullptr, *rs = nullptr, *cr = nullptr, *khat = nullptr;
+    bool needs_aux = false;  // a column transform keeps its plane outside shared memory
+    const void *exps = nullptr;  // ExpDesc<T>[nexp]
+    void *stats = nullptr;       // ExpStats[nexp]
+    unsigned long long *err = nullptr;
+    double *part_sum = nullptr, *red_sum = nullptr;
+    unsigned long long *part_neg = nullptr, *red_neg = nullptr;
 };
 
 std::unique_ptr<Engine> make_engine(const EngineOptions &opt);
+
+// Many independent fields (uneven grids and exposure counts) solved
+// together: every stage of an iteration is one persistent launch over the
+// work units of all fields, and the whole loop can run as one CUDA graph.
+struct BatchRecord {
+    double seconds = 0;                    // device time of the batch iteration
+    std::vector<double> signed_sum;        // per field
+    std::vector<uint64_t> negative;        // per field
+    std::vector<uint64_t> new_frozen, total_frozen;  // per exposure, fields in order
+};
+class Batch {
+  public:
+    virtual ~Batch() = default;
+    virtual void add_field(const std::string &manifest, int W, int H, int iw, int ih, int nexp, int transposed) = 0;
+    virtual void setup() = 0;
+    virtual void iterate(int n, bool check_each, std::vector<BatchRecord> *records) = 0;
+    virtual int fields() const = 0;
+    virtual Engine &field(int i) = 0;
+    virtual size_t units(int stage) const = 0;  // work units of a stage (diagnostics)
+};
+std::unique_ptr<Batch> make_batch(const EngineOptions &opt);
 
 // Smallest even / any 7-smooth integer >= n.
 int next_smooth(int n, bool even);

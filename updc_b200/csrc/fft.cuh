@@ -74,9 +74,16 @@ __host__ __device__ __forceinline__ int fpad_size(int count, int shift) { return
 // for the plan's stages (8-byte elements, NT threads, batch transforms).
 int fft_choose_padding(const FftPlan &plan, int nt, int cap, int batch);
 
+// Every split of n into radices no larger than rmax, each a non-increasing
+// sequence (the device's stage order), with at most `extra_stages` stages
+// more than the greedy split; the candidates the FFT autotuner times.
+void fft_factorizations(int n, int rmax, int extra_stages, std::vector<std::vector<int>> &out);
+
 // Builds the host twiddle table for n (complex, forward sign) and fills the
-// plan's stage fields.  The caller uploads the table and sets plan.tw.
+// plan's stage fields (greedy split, or the given radices in device order).
+// The caller uploads the table and sets plan.tw.
 template <typename T> std::vector<cx<T>> fft_make_table(int n, int rmax, FftPlan &plan);
+template <typename T> std::vector<cx<T>> fft_make_table(int n, const std::vector<int> &radices, FftPlan &plan);
 
 // ----------------------------------------------------------------------------- DFT kernels
 template <typename T> struct DftConst;

@@ -15,6 +15,22 @@ namespace updc {
 // compiled for two resident blocks per SM (64 registers a thread); FP64,
 // larger transforms and larger blocks for one (their butterflies need up to
 // 128 registers).
+// Threads per block of the spectral kernels: 512 (two blocks per SM) except
+// the FP32 adjoint column kernel, whose accumulator plane limits it to one
+// block per SM and which therefore runs 1024 threads (FP64 butterflies need
+// the 128-register budget of 512-thread blocks).
+constexpr int SPEC_NT = 512;
+template <typename T> struct SpecNtAdj {
+    static constexpr int value = sizeof(T) == 4 ? 1024 : 512;
+};
+constexpr size_t SPEC_SMEM_LIMIT = 227 * 1024;
+// Shared-memory capacity (complex elements) of the FFT instantiations.
+template <typename T> struct SpecCaps {
+    static constexpr int ROW = 5632;
+    static constexpr int COL_S = 5632;
+    static constexpr int COL_L = 11264;
+};
+
 template <int NT, int CAP, typename T> struct MinBlocks {
     static constexpr int value = (NT <= 512 && CAP <= 5632 && sizeof(T) == 4) ? 2 : 1;
 };
@@ -33,8 +49,8 @@ template <typename T> struct PlaneLoader {
 // Centre-wrapped, normalised PSF on the FW x FH grid (updc_core.c:813-821):
 // PSF pixel (x, y) goes to ((x - fw/2) mod FW, (y - fh/2) mod FH); with
 // transposed storage the source index is x*pw + y.
-template <typename T> struct PsfLoader {
-    const float *psf;
+template <typename T, typename P = float> struct PsfLoader {
+    const P *psf;
     int pw, fwid, fhei, FW, FH, transposed;
     T inv;
     __device__ __forceinline__ T operator()(int, int yy, int xx) const {
@@ -79,16 +95,15 @@ __host__ __device__ inline size_t row_stage_bytes(int B, int M, size_t csize) {
 // transformed along x with an M-point complex FFT of z[m] = x[2m] + i x[2m+1]
 // and the split z -> X post-processing; bins are stored u-major.  Exposure =
 // blockIdx.y.
+// One block's tile: rows [y0, y0 + B) of plane `kexp`.  The block-level
+// body shared by the single-field kernel and the batched one (batch.cuh).
 template <typename T, int NT, int CAP, class Loader, bool TMA>
-__global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
-    k_row_r2c(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ post, Loader ld, int W, int rows, int B,
-              FastDiv bdiv, SpecRef out, const __grid_constant__ CUtensorMap omap) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+__device__ __forceinline__ void row_r2c_tile(const FftPlan &plan, const cx<T> *__restrict__ post, const Loader &ld,
+                                             int W, int rows, int B, FastDiv bdiv, SpecRef out,
+                                             const CUtensorMap *omap, int y0, int kexp, unsigned char *smem_raw) {
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
     const int M = plan.n, sh = plan.pad_shift;
-    const int y0 = blockIdx.x * B;
     const int nb = min(B, rows - y0);
-    const int kexp = blockIdx.y;
     for (int b = 0; b < B; ++b)
         for (int m = threadIdx.x; m < M; m += NT) {
             T a = 0, c = 0;
@@ -126,10 +141,19 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
             constexpr int EW = TmaElems<T>::value;
             const int ub = row_ubox(M);
             for (int bx = 0; bx < row_nbox(M); ++bx)
-                tma_store_3d(&omap, stage + (size_t)bx * ub * B, y0 * EW, bx * ub, kexp);
+                tma_store_3d(omap, stage + (size_t)bx * ub * B, y0 * EW, bx * ub, kexp);
             tma_store_commit_and_wait();
         }
     }
+}
+
+template <typename T, int NT, int CAP, class Loader, bool TMA>
+__global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
+    k_row_r2c(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ post, Loader ld, int W, int rows, int B,
+              FastDiv bdiv, SpecRef out, const __grid_constant__ CUtensorMap omap) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    row_r2c_tile<T, NT, CAP, Loader, TMA>(plan, post, ld, W, rows, B, bdiv, out, &omap, blockIdx.x * B, blockIdx.y,
+                                          smem_raw);
 }
 
 // ---------------------------------------------------------------------------- row C2R
@@ -147,17 +171,14 @@ template <typename T> struct PlaneStore {
 // The imaginary parts of the DC and Nyquist bins are ignored, as FFTW does.
 // With TMA the block's {B rows} x {all u} tile arrives through the tensor map.
 template <typename T, int NT, int CAP, class Epi, bool TMA>
-__global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
-    k_row_c2r(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ post, SpecRef in,
-              const __grid_constant__ CUtensorMap imap, int rows, int W, int B, FastDiv bdiv, T scale, Epi epi,
-              unsigned long long *__restrict__ err) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+__device__ __forceinline__ void row_c2r_tile(const FftPlan &plan, const cx<T> *__restrict__ post, SpecRef in,
+                                             const CUtensorMap *imap, int rows, int W, int B, FastDiv bdiv, T scale,
+                                             const Epi &epi, unsigned long long *__restrict__ err, int y0, int kexp,
+                                             unsigned char *smem_raw) {
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
     __shared__ __align__(8) uint64_t bar;
     const int M = plan.n, sh = plan.pad_shift;
-    const int y0 = blockIdx.x * B;
     const int nb = min(B, rows - y0);
-    const int kexp = blockIdx.y;
     cx<T> *stage = reinterpret_cast<cx<T> *>(smem_raw + row_buf_bytes(B, M, sizeof(cx<T>), sh));
     const cx<T> *src = reinterpret_cast<const cx<T> *>(in.p) + kexp * in.batch_stride;
     if (TMA) {
@@ -168,7 +189,7 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
             const int nbox = row_nbox(M), ub = row_ubox(M);
             mbar_arrive_expect_tx(&bar, (uint32_t)row_stage_bytes(B, M, sizeof(cx<T>)));
             for (int bx = 0; bx < nbox; ++bx)
-                tma_load_3d(stage + (size_t)bx * ub * B, &imap, &bar, y0 * EW, bx * ub, kexp);
+                tma_load_3d(stage + (size_t)bx * ub * B, imap, &bar, y0 * EW, bx * ub, kexp);
         }
         if (!mbar_wait_bounded(&bar, 0)) {
             if (threadIdx.x == 0)
@@ -206,6 +227,16 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
         }
 }
 
+template <typename T, int NT, int CAP, class Epi, bool TMA>
+__global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
+    k_row_c2r(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ post, SpecRef in,
+              const __grid_constant__ CUtensorMap imap, int rows, int W, int B, FastDiv bdiv, T scale, Epi epi,
+              unsigned long long *__restrict__ err) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    row_c2r_tile<T, NT, CAP, Epi, TMA>(plan, post, in, &imap, rows, W, B, bdiv, scale, epi, err, blockIdx.x * B,
+                                       blockIdx.y, smem_raw);
+}
+
 
 // ---------------------------------------------------------------------------- columns
 // Forward model for every exposure from the estimate's row-pass intermediate:
@@ -216,14 +247,12 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
 // conj(FFT(conj(.))), which keeps a single inlined copy of the FFT (two
 // copies make ptxas spill).
 template <typename T, int NT, int CAP>
-__global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_forward(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ rx, int ldr, int rows_in,
-                                                    const cx<T> *__restrict__ khat, size_t khat_stride, int nexp,
-                                                    cx<T> *__restrict__ y, int ldy, size_t y_stride, int rows_out,
-                                                    int nu, cx<T> *aux) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void col_forward_column(const FftPlan &plan, const cx<T> *__restrict__ rx, int ldr,
+                                                   int rows_in, const cx<T> *__restrict__ khat, size_t khat_stride,
+                                                   int nexp, cx<T> *__restrict__ y, int ldy, size_t y_stride,
+                                                   int rows_out, cx<T> *aux, int u, unsigned char *smem_raw) {
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
     const int n = plan.n, sh = plan.pad_shift;
-    const int u = blockIdx.x;
     cx<T> *xh = aux ? aux + (size_t)u * n : reinterpret_cast<cx<T> *>(smem_raw + fft_buf_bytes(n, sizeof(cx<T>), sh));
     const cx<T> *src = rx + (size_t)u * ldr;
 #pragma unroll 1
@@ -250,7 +279,17 @@ __global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_forw
         }
         __syncthreads();
     }
+}
+
+template <typename T, int NT, int CAP>
+__global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_forward(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ rx, int ldr, int rows_in,
+                                                    const cx<T> *__restrict__ khat, size_t khat_stride, int nexp,
+                                                    cx<T> *__restrict__ y, int ldy, size_t y_stride, int rows_out,
+                                                    int nu, cx<T> *aux) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     (void)nu;
+    col_forward_column<T, NT, CAP>(plan, rx, ldr, rows_in, khat, khat_stride, nexp, y, ldy, y_stride, rows_out, aux,
+                                   blockIdx.x, smem_raw);
 }
 
 // Cross-exposure accumulation policies for the adjoint sum
@@ -299,13 +338,12 @@ struct AccKahan {  // FP32 products, Kahan-compensated FP32 sum
 // the final inverse goes through the same forward-FFT call site as
 // conj(FFT(conj(.))).
 template <typename T, class Acc, int NT, int CAP>
-__global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_adjoint(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ rs, int ldr, size_t rs_stride,
-                                                    int rows_in, const cx<T> *__restrict__ khat, size_t khat_stride, int nexp,
-                                                    cx<T> *__restrict__ c, int ldc, int rows_out, typename Acc::S *aux) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void col_adjoint_column(const FftPlan &plan, const cx<T> *__restrict__ rs, int ldr,
+                                                   size_t rs_stride, int rows_in, const cx<T> *__restrict__ khat,
+                                                   size_t khat_stride, int nexp, cx<T> *__restrict__ c, int ldc,
+                                                   int rows_out, typename Acc::S *aux, int u, unsigned char *smem_raw) {
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
     const int n = plan.n, sh = plan.pad_shift;
-    const int u = blockIdx.x;
     typename Acc::S *acc = aux ? aux + (size_t)u * n
                                : reinterpret_cast<typename Acc::S *>(smem_raw + fft_buf_bytes(n, sizeof(cx<T>), sh));
     for (int v = threadIdx.x; v < n; v += NT) Acc::zero(acc[v]);
@@ -334,6 +372,15 @@ __global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_adjo
         }
         __syncthreads();
     }
+}
+
+template <typename T, class Acc, int NT, int CAP>
+__global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_adjoint(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ rs, int ldr, size_t rs_stride,
+                                                    int rows_in, const cx<T> *__restrict__ khat, size_t khat_stride, int nexp,
+                                                    cx<T> *__restrict__ c, int ldc, int rows_out, typename Acc::S *aux) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    col_adjoint_column<T, Acc, NT, CAP>(plan, rs, ldr, rs_stride, rows_in, khat, khat_stride, nexp, c, ldc, rows_out,
+                                        aux, blockIdx.x, smem_raw);
 }
 
 // Plain column transform (setup: PSF spectra and generic 2-D transforms).

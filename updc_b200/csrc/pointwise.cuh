@@ -84,20 +84,18 @@ template <typename T> struct LinkSum {
 // prediction is accumulated in FP64 and raw_mu is rounded once from the FP64
 // sum with the offset, so the FreezeMu threshold is decided on a compensated
 // raw_mu.
+// Block `block` of `nblocks` over exposure k's pixels (grid-stride); the
+// body of k_detector and of the batched detector (batch.cuh).
 template <typename T, bool COMP>
-__global__ void __launch_bounds__(DET_WARPS * 32) k_detector(const ExpDesc<T> *__restrict__ exps, size_t nin, size_t nout,
-                                                           const T *__restrict__ blur_all, T *__restrict__ wr_all,
-                                                           ExpStats *__restrict__ stats, unsigned long long *__restrict__ err) {
+__device__ __forceinline__ void detector_tiles(const ExpDesc<T> &e, int k, size_t nin, const T *__restrict__ blur,
+                                               T *__restrict__ wr, ExpStats *__restrict__ stats,
+                                               unsigned long long *__restrict__ err, unsigned block, unsigned nblocks) {
     __shared__ uint32_t s_idx[DET_WARPS][DET_LCAP];
     __shared__ float s_frac[DET_WARPS][DET_LCAP];
-    const int k = blockIdx.y;
-    const ExpDesc<T> e = exps[k];
-    const T *blur = blur_all + k * nout;
-    T *wr = wr_all + k * nin;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned long long nnew = 0, ntot = 0, mn = ~0ull;
-    const size_t step = (size_t)gridDim.x * DET_WARPS * 32;
-    for (size_t p0 = ((size_t)blockIdx.x * DET_WARPS + warp) * 32; p0 < nin; p0 += step) {
+    const size_t step = (size_t)nblocks * DET_WARPS * 32;
+    for (size_t p0 = ((size_t)block * DET_WARPS + warp) * 32; p0 < nin; p0 += step) {
         const size_t p = p0 + lane;
         const bool valid = p < nin;
         // every per-pixel load first (independent of each other)
@@ -210,20 +208,25 @@ __global__ void __launch_bounds__(DET_WARPS * 32) k_detector(const ExpDesc<T> *_
     }
 }
 
+template <typename T, bool COMP>
+__global__ void __launch_bounds__(DET_WARPS * 32) k_detector(const ExpDesc<T> *__restrict__ exps, size_t nin, size_t nout,
+                                                           const T *__restrict__ blur_all, T *__restrict__ wr_all,
+                                                           ExpStats *__restrict__ stats, unsigned long long *__restrict__ err) {
+    const int k = blockIdx.y;
+    const ExpDesc<T> e = exps[k];
+    detector_tiles<T, COMP>(e, k, nin, blur_all + k * nout, wr_all + k * nin, stats, err, blockIdx.x, gridDim.x);
+}
+
 // ---------------------------------------------------------------------------- adjoint gather
 // scatter_k[t] = sum over the transposed entries of t, in increasing source
 // pixel order, of fmaf(frac, value[p], acc): the exact sequence of
 // updc_core.c:1173-1176 for target t.  ACC may be wider than T.  Entries are
 // read in chunks: all loads of a chunk first, then the ordered fma chain.
 template <typename T, typename ACC, typename V>
-__global__ void __launch_bounds__(256) k_scatter_t(const ExpDesc<T> *__restrict__ exps, size_t nin, size_t nout,
-                                                   const V *__restrict__ val_all, int use_weight, ACC *__restrict__ out_all) {
-    const int k = blockIdx.y;
-    const ExpDesc<T> e = exps[k];
-    const V *val = use_weight ? nullptr : val_all + k * nin;
-    ACC *out = out_all + k * nout;
+__device__ __forceinline__ void scatter_targets(const ExpDesc<T> &e, size_t nout, const V *__restrict__ val,
+                                                int use_weight, ACC *__restrict__ out, unsigned block, unsigned nblocks) {
     constexpr int CH = 4;
-    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nout; t += (size_t)gridDim.x * blockDim.x) {
+    for (size_t t = block * (size_t)blockDim.x + threadIdx.x; t < nout; t += (size_t)nblocks * blockDim.x) {
         const uint32_t a = e.toff[t], b = e.toff[t + 1];
         ACC acc = ACC(0);
         for (uint32_t ic = a; ic < b; ic += CH) {
@@ -257,16 +260,26 @@ __global__ void __launch_bounds__(256) k_scatter_t(const ExpDesc<T> *__restrict_
     }
 }
 
+template <typename T, typename ACC, typename V>
+__global__ void __launch_bounds__(256) k_scatter_t(const ExpDesc<T> *__restrict__ exps, size_t nin, size_t nout,
+                                                   const V *__restrict__ val_all, int use_weight, ACC *__restrict__ out_all) {
+    const int k = blockIdx.y;
+    const ExpDesc<T> e = exps[k];
+    scatter_targets<T, ACC, V>(e, nout, use_weight ? nullptr : val_all + k * nin, use_weight, out_all + k * nout,
+                               blockIdx.x, gridDim.x);
+}
+
 // ---------------------------------------------------------------------------- update
 // updc_core.c:1437-1456, with per-block partial sums for the diagnostics.
 template <typename T>
-__global__ void __launch_bounds__(256) k_update(size_t nout, const T *__restrict__ corr, const T *__restrict__ den,
-                                                T *__restrict__ x, T max_sens, unsigned long long *__restrict__ err,
-                                                double *__restrict__ part_sum, unsigned long long *__restrict__ part_neg) {
+__device__ __forceinline__ void update_block(size_t nout, const T *__restrict__ corr, const T *__restrict__ den,
+                                             T *__restrict__ x, T max_sens, unsigned long long *__restrict__ err,
+                                             double *__restrict__ part_sum, unsigned long long *__restrict__ part_neg,
+                                             unsigned block, unsigned nblocks) {
     double sum = 0.0;
     unsigned long long neg = 0;
     const T thr = mul_rn((T)-1.0e-6f, max_sens);
-    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nout; t += (size_t)gridDim.x * blockDim.x) {
+    for (size_t t = block * (size_t)blockDim.x + threadIdx.x; t < nout; t += (size_t)nblocks * blockDim.x) {
         const T d = den[t];
         T v = x[t];
         if (d > (T)1e-8f) {
@@ -302,14 +315,21 @@ __global__ void __launch_bounds__(256) k_update(size_t nout, const T *__restrict
             a += s_sum[i];
             b += s_neg[i];
         }
-        part_sum[blockIdx.x] = a;
-        part_neg[blockIdx.x] = b;
+        part_sum[block] = a;
+        part_neg[block] = b;
     }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256) k_update(size_t nout, const T *__restrict__ corr, const T *__restrict__ den,
+                                                T *__restrict__ x, T max_sens, unsigned long long *__restrict__ err,
+                                                double *__restrict__ part_sum, unsigned long long *__restrict__ part_neg) {
+    update_block<T>(nout, corr, den, x, max_sens, err, part_sum, part_neg, blockIdx.x, gridDim.x);
+}
+
 // Fixed-order final reduction of per-block partials (deterministic).
-static __global__ void k_reduce_partials(const double *part_sum, const unsigned long long *part_neg, int n, double *out_sum,
-                                  unsigned long long *out_neg) {
+__device__ __forceinline__ void reduce_partials_block(const double *part_sum, const unsigned long long *part_neg, int n,
+                                                      double *out_sum, unsigned long long *out_neg) {
     __shared__ double s[256];
     __shared__ unsigned long long c[256];
     double a = 0;
@@ -332,6 +352,10 @@ static __global__ void k_reduce_partials(const double *part_sum, const unsigned 
         *out_sum = s[0];
         *out_neg = c[0];
     }
+}
+static __global__ void k_reduce_partials(const double *part_sum, const unsigned long long *part_neg, int n, double *out_sum,
+                                         unsigned long long *out_neg) {
+    reduce_partials_block(part_sum, part_neg, n, out_sum, out_neg);
 }
 
 // ---------------------------------------------------------------------------- setup
@@ -373,13 +397,14 @@ static __global__ void k_weight_sample(size_t nin, const float *__restrict__ wht
 }
 
 // PSF validity and FP64 sum (fixed-order block tree; deterministic).
-static __global__ void k_psf_sum_f64(const float *__restrict__ psf, size_t n, double *__restrict__ partial,
+template <typename P>
+__global__ void k_psf_sum_f64(const P *__restrict__ psf, size_t n, double *__restrict__ partial,
                               unsigned long long *__restrict__ err) {
     __shared__ double s[256];
     double a = 0.0;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const float v = psf[i];
-        if (!isfinite(v) || v < 0.0f) record_error(err, STAGE_SETUP, i, ERR_INVALID_PSF_PIXEL);
+        const P v = psf[i];
+        if (!isfinite(v) || v < P(0)) record_error(err, STAGE_SETUP, i, ERR_INVALID_PSF_PIXEL);
         a += (double)v;
     }
     s[threadIdx.x] = a;

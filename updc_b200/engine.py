@@ -48,7 +48,8 @@ class Engine:
 
     def __init__(self, form: str = "fp32", device: int = 0, use_graph: bool = True,
                  reuse_links: bool = True, compensated_mu: Optional[bool] = None, verbose: bool = False,
-                 fft_shape: Optional[tuple] = None, stage_timing: bool = False):
+                 fft_shape: Optional[tuple] = None, stage_timing: bool = False, autotune: bool = False,
+                 retune: bool = False, tune_cache_dir: Optional[str] = None):
         L = _lib.load()
         opt = _lib.Options()
         L.updc_default_options(ctypes.byref(opt))
@@ -59,6 +60,10 @@ class Engine:
         opt.compensated_mu = -1 if compensated_mu is None else int(bool(compensated_mu))
         opt.verbose = 1 if verbose else 0
         opt.stage_timing = 1 if stage_timing else 0
+        opt.autotune = 1 if autotune else 0
+        opt.retune = 1 if retune else 0
+        self._cache_dir = str(tune_cache_dir).encode() if tune_cache_dir else None
+        opt.tune_cache_dir = self._cache_dir
         if fft_shape:
             opt.fft_width, opt.fft_height = fft_shape
         h = ctypes.c_void_p()
@@ -161,6 +166,18 @@ class Engine:
     def fft_shape(self) -> tuple:
         return int(self.scalar(2)), int(self.scalar(3))
 
+    def fft_radices(self, axis: int) -> List[int]:
+        """Radix split of the row (axis 0, FW/2 points) or column (axis 1, FH points) transform."""
+        buf = (ctypes.c_int * 32)()
+        n = ctypes.c_int()
+        check(self._L.updc_fft_radices(self._h, axis, buf, 32, ctypes.byref(n)))
+        return list(buf[:n.value])
+
+    @property
+    def autotune_info(self) -> dict:
+        return {"seconds": self.scalar(7), "plans_timed": int(self.scalar(8)), "cache_hit": bool(self.scalar(9)),
+                "modelled_ms": self.scalar(10)}
+
     @property
     def masked_pixels(self) -> int:
         return int(self.scalar(4))
@@ -188,6 +205,44 @@ class Engine:
         n = ctypes.c_uint64()
         check(self._L.updc_stage_update(self._h, ctypes.byref(s), ctypes.byref(n)))
         return s.value, int(n.value)
+
+    # ------------------------------------------------------------------ differentiable model
+    def set_exposure_offsets(self, exposure: int, background: float, pedestal: float) -> None:
+        check(self._L.updc_set_exposure_offsets(self._h, exposure, float(background), float(pedestal)))
+
+    def set_psf(self, exposure: int, psf: np.ndarray) -> None:
+        """Replace an exposure's PSF (2-D float32 or float64 array, manifest layout)."""
+        a = np.ascontiguousarray(psf, np.float64 if psf.dtype == np.float64 else np.float32)
+        check(self._L.updc_set_psf(self._h, exposure, a.ctypes.data, a.shape[1], a.shape[0],
+                                   1 if a.dtype == np.float64 else 0))
+
+    def nll(self) -> np.ndarray:
+        """Forward model of the current estimate; per exposure
+        [L_k, sum r, sum W log mu, pixels left out] (see updc_nll)."""
+        out = np.zeros((self.nexp, 4), np.float64)
+        check(self._L.updc_nll(self._h, out.ctypes.data))
+        return out
+
+    def nll_partials(self) -> np.ndarray:
+        """Per-block partial sums behind the last nll(): (exposures, blocks, 4)."""
+        n = ctypes.c_size_t()
+        check(self._L.updc_nll_partials(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, np.float64)
+        check(self._L.updc_nll_partials(self._h, out.ctypes.data, n.value, ctypes.byref(n)))
+        return out.reshape(self.nexp, -1, 4)
+
+    def nll_adjoint(self) -> None:
+        check(self._L.updc_nll_adjoint(self._h))
+
+    def psf_gradient(self, exposure: int, shape: tuple) -> np.ndarray:
+        out = np.zeros(shape, np.float64)
+        check(self._L.updc_psf_gradient(self._h, exposure, out.ctypes.data))
+        return out
+
+    def copy_plane_device(self, name: str, ptr: int, to_engine: bool, as_double: bool, exposure: int = 0,
+                          stream: int = 0) -> None:
+        check(self._L.updc_copy_plane_device(self._h, PLANES[name], exposure, ptr, 1 if to_engine else 0,
+                                             1 if as_double else 0, stream or None))
 
     # ------------------------------------------------------------------ LinkMaps
     def link_count(self, exposure: int) -> int:

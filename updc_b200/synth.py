@@ -335,3 +335,34 @@ def generate(name_or_workload, directory: os.PathLike, use_torch: Optional[bool]
     manifest = d / "manifest.txt"
     write_manifest(manifest, rows)
     return Dataset(w, d, manifest, rows)
+
+
+# ----------------------------------------------------------------------------- batched cutouts
+BATCH_GRIDS = (128, 192, 256, 384, 512, 768)
+
+
+def batch_workloads(n_fields: int = 64, seed: int = 2, iterations: int = 30) -> List[Workload]:
+    """Independent cutout fields: target grid uniform over BATCH_GRIDS (square),
+    3-12 exposures of target/2 +- 16 detector pixels at scale 2 with random
+    affine maps and dithers as in c0, Gaussian+Moffat PSFs of 33-129 px with a
+    core width of 1.0-1.6 px; scene density as c0 per unit area."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_fields):
+        t = int(rng.choice(BATCH_GRIDS))
+        nexp = int(rng.integers(3, 13))
+        det = t // 2 + int(rng.integers(-16, 17))
+        psf = 2 * int(rng.integers(16, 65)) + 1
+        area = (t / 256.0) ** 2
+        out.append(Workload(f"field{i:02d}", t, t, det, det, nexp, psf, "gauss_moffat",
+                            max(4, int(40 * area)), max(1, int(10 * area)), iterations,
+                            psf_sigma=float(rng.uniform(1.0, 1.6)), seed=1000 + i))
+    return out
+
+
+def generate_batch(directory: os.PathLike, n_fields: int = 64, seed: int = 2,
+                   iterations: int = 30) -> List[Dataset]:
+    """Write one handoff file set per field under ``directory/<field name>``."""
+    d = Path(directory)
+    return [generate(w, d / w.name, use_torch=False) for w in batch_workloads(n_fields, seed, iterations)]
+
