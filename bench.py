@@ -11,8 +11,11 @@ estimate uploaded from and read back to host memory every step.  The per-stage
 event timing pass gives the dominant kernel's roofline.  ``--impl reference``
 times the reference core itself (compiled from its sources with the FFTW-API
 shim, oracle/_ref) on the host cores for the same workload.
-Under torchrun (N > 1) every rank solves its own field (replicas: the path of
-one field does not shard without a collective).
+Under torchrun (N > 1) the field's exposures are split over the ranks: each
+rank computes the partial correction of its exposures, one NCCL all-reduce
+sums them and every rank applies the same update (strong scaling; --replicas
+runs N independent copies instead).  ``--workload c2`` runs 64 batched
+cutout fields, every stage one persistent launch over all fields.
 """
 from __future__ import annotations
 
@@ -121,6 +124,14 @@ def stage_bytes(w, fw, fh, links, tlinks, dtype_bytes=4):
         "update": 4 * nout * r,
     }
 
+
+# DRAM bytes (read + write) over algorithmic bytes per spectral stage, from
+# the full-set ncu capture of the same kernels on c3 (4 x 1024^2 -> 2048^2,
+# FFT 3584^2): the kernels' traffic grows in proportion to the columns, rows
+# and exposures they process, so this ratio carries a capture of the small
+# case to the benchmark's workload.
+TRAFFIC_RATIO_C3 = {"estimate_x_pass": 18.4 / 46.2, "forward_y_passes": 322.0 / 352.5, "forward_x_pass": 155.2 / 184.6,
+                    "scatter_x_pass": 134.5 / 184.6, "adjoint_y_x_passes": (349.1 + 29.6) / (352.5 + 46.2)}
 
 STAGES = ["estimate_x_pass", "forward_y_passes", "forward_x_pass", "detector", "adjoint_gather",
           "scatter_x_pass", "adjoint_y_x_passes", "update"]
@@ -258,6 +269,163 @@ def fp64_comparison(eng, ds, w, args, device):
             "fp64_ms_per_iteration": round(ms64, 4)}
 
 
+def batch_arm(args, rank, world, local_rank):
+    """Batched cutouts: 64 fields of uneven size and exposure count, every
+    stage one persistent launch over all fields, the loop one CUDA graph.
+    A step is one iteration of every field; beside it, the same fields
+    solved one after another by their own engines (graph per iteration)."""
+    import torch
+    from updc_b200 import synth
+    from updc_b200.batch import Batch
+    from updc_b200.engine import Engine
+    torch.cuda.set_device(local_rank)
+    workdir = Path(args.data_dir or tempfile.mkdtemp(prefix=f"updc_bench_batch_r{rank}_"))
+    t0 = time.time()
+    data = synth.generate_batch(workdir, n_fields=args.fields)
+    gen_s = time.time() - t0
+    b = Batch(form=args.form, device=local_rank, autotune=not args.no_autotune, tune_cache_dir=workdir)
+    for ds in data:
+        w = ds.workload
+        b.add_field(ds.manifest, w.W, w.H, w.iw, w.ih, w.nexp)
+    t0 = time.time()
+    b.setup()
+    setup_s = time.time() - t0
+    b.iterate(args.warmup)
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        recs = b.iterate(args.steps)
+        torch.cuda.synchronize()
+    ms = 1000.0 * sum(r["seconds"] for r in recs) / len(recs)
+    # the same fields, one engine each, run one after another
+    seq_ms = 0.0
+    for ds in data:
+        w = ds.workload
+        e = Engine(form=args.form, device=local_rank, autotune=not args.no_autotune, tune_cache_dir=workdir)
+        e.load(str(ds.manifest), w.W, w.H, w.iw, w.ih, w.nexp).setup()
+        e.iterate(args.warmup, check_each=False)
+        st = e.iterate(args.steps, check_each=False)
+        seq_ms += 1000.0 * sum(x.seconds for x in st) / len(st)
+        e.close()
+    # e2e: upload every field's estimate from pinned host memory, one batch
+    # iteration, read every estimate back
+    hosts = []
+    for i in range(b.fields):
+        f = b.field(i)
+        hosts.append(torch.empty((f.H, f.W), dtype=torch.float64 if args.form == "fp64" else torch.float32,
+                                 pin_memory=True).numpy())
+        f.read_plane_into("estimate", hosts[-1])
+    e2e_steps = max(2, min(args.steps, 5))
+    t0 = time.time()
+    for _ in range(e2e_steps):
+        for i in range(b.fields):
+            b.field(i).set_plane("estimate", hosts[i])
+        b.iterate(1, check_each=True)
+        for i in range(b.fields):
+            b.field(i).read_plane_into("estimate", hosts[i])
+    e2e_ms = 1000.0 * (time.time() - t0) / e2e_steps
+    nbytes = sum(h.nbytes for h in hosts)
+    result = {
+        "metric": "ms/iteration (all fields)", "value": round(ms, 4), "unit": "ms", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32", "data": "synthetic",
+        "config": {"workload": "c2", "fields": b.fields, "exposures": int(sum(d.workload.nexp for d in data)),
+                   "grids": sorted({d.workload.W for d in data}), "form": args.form,
+                   "units": {s: b.units(i) for i, s in enumerate(["estimate_rows", "columns", "forward_rows",
+                                                                   "detector", "adjoint_gather", "scatter_rows",
+                                                                   "update", "adjoint_rows"])},
+                   "graph": "whole loop of --steps iterations", "l2": "per-field planes re-read each stage"},
+        "sequential_single_field_ms": round(seq_ms, 4),
+        "speedup_vs_sequential": round(seq_ms / ms, 3),
+        "setup_s": round(setup_s, 2), "generate_s": round(gen_s, 1),
+        "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
+        "gpu_launches": 11 * args.steps,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(result))
+    b.close()
+    if not args.data_dir:
+        shutil.rmtree(workdir, ignore_errors=True)
+    return 0
+
+
+def sharded_arm(args, rank, world, local_rank):
+    """N > 1: one field, its exposures split over the ranks (contiguous
+    shares), every rank set up on the whole field; per iteration each rank
+    computes the partial correction of its exposures, one NCCL all-reduce
+    sums them, and every rank applies the same update.  Total work is fixed
+    (strong scaling); time is the max over ranks of the device-timed loop."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from updc_b200 import synth
+    from updc_b200.sharded import ShardedSolver, open_engine_shard
+    torch.cuda.set_device(local_rank)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                            device_id=torch.device("cuda", local_rank))
+    w = synth.WORKLOADS[args.workload]
+    workdir = Path(args.data_dir or tempfile.mkdtemp(prefix=f"updc_bench_shard_r{rank}_"))
+    try:
+        ds = synth.generate(w.name, workdir, use_torch=True)
+        t0 = time.time()
+        shard = open_engine_shard(str(ds.manifest), w.W, w.H, w.iw, w.ih, w.nexp, rank, world, form=args.form,
+                                  device=local_rank)
+        solver = ShardedSolver(shard, dist)
+        setup_s = time.time() - t0
+        solver.iterate(args.warmup)
+        dist.barrier()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        with ClockSampler(local_rank) as clocks:
+            ev[0].record()
+            recs = solver.iterate(args.steps)
+            ev[1].record()
+            torch.cuda.synchronize()
+        t = torch.tensor([ev[0].elapsed_time(ev[1]) / args.steps], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        # e2e: every step the estimate comes from pinned host memory and goes back
+        eng = shard.engine
+        x = torch.empty((w.H, w.W), dtype=torch.float64 if args.form == "fp64" else torch.float32,
+                        pin_memory=True).numpy()
+        eng.read_plane_into("estimate", x)
+        e2e_steps = max(2, min(args.steps, 5))
+        dist.barrier()
+        t0 = time.time()
+        for _ in range(e2e_steps):
+            eng.set_plane("estimate", x)
+            solver.iterate(1)
+            eng.read_plane_into("estimate", x)
+        te = torch.tensor([1000.0 * (time.time() - t0) / e2e_steps], device="cuda")
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        first, count = shard.first, shard.count
+        result = {
+            "metric": "ms/iteration", "value": round(ms, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": False, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "form": args.form, "target": [w.W, w.H], "exposures": w.nexp,
+                       "detector": [w.iw, w.ih], "psf": w.psf_size, "fft": list(eng.fft_shape),
+                       "parallelism": f"exposure shards over {world} ranks, NCCL all-reduce of the correction plane",
+                       "rank0_exposures": [first, first + count],
+                       "l2": "working set >> 126 MB L2; no flush needed"},
+            "setup_s": round(setup_s, 2),
+            "signed_sum_last": recs[-1]["signed_sum"],
+            "e2e": {"value": round(float(te.item()), 3), "unit": "ms", "h2d_bytes_per_step": x.nbytes,
+                    "d2h_bytes_per_step": x.nbytes},
+            "gpu_launches": (10 + 4) * args.steps,
+            "clocks": clocks.summary(),
+        }
+        if rank == 0:
+            print(json.dumps(result))
+        eng.close()
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+        if not args.data_dir:
+            shutil.rmtree(workdir, ignore_errors=True)
+    return 0
+
+
 def b200_arm(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -326,7 +494,10 @@ def b200_arm(args, rank, world, local_rank):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(ds, w)
-    launches_per_iter = 9 + w.nexp
+    # estimate R2C, column forward, forward C2R (all exposures), detector,
+    # adjoint gather, scatter R2C (all exposures), column adjoint, adjoint
+    # C2R, update, reduction
+    launches_per_iter = 10
     result = {
         "metric": "ms/iteration", "value": round(ms, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": False,
@@ -344,7 +515,9 @@ def b200_arm(args, rank, world, local_rank):
         "stage_gbs": {k: round(sb[k] / (stage_ms[k] * 1e-3) / 1e9, 1) for k in STAGES},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                     "algorithmic_bytes": sb[dom], "traffic": None},
+                     "algorithmic_bytes": sb[dom],
+                     "traffic": round(sb[dom] * TRAFFIC_RATIO_C3[dom]) if dom in TRAFFIC_RATIO_C3 else None,
+                     "traffic_source": "ncu dram__bytes_read+write of the c3 capture, scaled by units processed"},
         "cpu_baseline": cpu,
         "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": x.itemsize * nout,
                 "d2h_bytes_per_step": x.itemsize * nout},
@@ -375,6 +548,9 @@ def main():
     p.add_argument("--form", default="fp32", choices=["fp32", "fp64", "fp32-kahan", "fp32-reference"])
     p.add_argument("--data-dir", default=None)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--replicas", action="store_true",
+                   help="with N > 1: N independent replicas instead of exposure shards of one field")
+    p.add_argument("--fields", type=int, default=64, help="fields of the batched workload (c2)")
     p.add_argument("--no-autotune", action="store_true",
                    help="smallest 7-smooth FFT shape and greedy radix splits instead of the device autotuner")
     p.add_argument("--no-fp64-check", action="store_true",
@@ -383,6 +559,10 @@ def main():
     rank, world, local_rank = env_rank()
     if args.impl == "reference":
         return reference_arm(args, rank, world)
+    if args.workload == "c2":
+        return batch_arm(args, rank, world, local_rank)
+    if world > 1 and not args.replicas:
+        return sharded_arm(args, rank, world, local_rank)
     return b200_arm(args, rank, world, local_rank)
 
 

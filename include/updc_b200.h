@@ -168,6 +168,25 @@ int updc_psf_gradient(updc_engine *h, int exposure, double *out);
 int updc_copy_plane_device(updc_engine *h, int which, int exposure, void *device_ptr, int to_engine, int as_double,
                            void *stream);
 
+/* Exposure shards (multi-GPU solve of one field; no reference counterpart,
+ * the reference runs one process): after updc_setup on the whole field,
+ * iterate only exposures [first, first + count).  A rank then runs
+ * updc_stage_forward / _detector / _correction for its shard, sums the
+ * CORRECTION plane over ranks (the one exchange of the iteration,
+ * updc_core.c:1280-1287 split by exposure), writes it back and runs
+ * updc_stage_update.  updc_refresh_sensitivity recomputes max_sensitivity
+ * after the DENOMINATOR plane was replaced. */
+int updc_set_active_exposures(updc_engine *h, int first, int count);
+int updc_refresh_sensitivity(updc_engine *h);
+
+/* Checkpoint / resume (no reference counterpart: the reference writes the
+ * estimate only, core:1460-1470).  updc_save_state writes the estimate and the
+ * persistent FreezeMu masks with an iteration count; updc_load_state, on an
+ * engine set up from the same manifest and form, restores them, so the next
+ * iterations continue the saved run exactly. */
+int updc_save_state(updc_engine *h, const char *path, uint64_t iteration);
+int updc_load_state(updc_engine *h, const char *path, uint64_t *iteration);
+
 /* LinkMap v2 (updc_core.c:40-79, 463-496, 530-609, 645-662). */
 uint64_t updc_link_count(updc_engine *h, int exposure);
 int updc_link_encoding(updc_engine *h, int exposure);

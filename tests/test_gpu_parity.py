@@ -110,6 +110,26 @@ def test_forward_model_vs_fp64_oracle(engine_lib, oracle, datasets, form, tol):
         assert rel_rms(e.plane("blur", k, as_double=True), ref) <= tol
 
 
+@pytest.mark.parametrize("form,tol", [("fp32", 2e-6), ("fp64", 1e-12)])
+def test_large_column_transforms(engine_lib, oracle, datasets, form, tol):
+    """FFT heights above the small column capacity (the 11264-point kernels;
+    FP64 keeps X-hat and the adjoint accumulator in global memory): forward
+    model and two iterations against the FP64 oracle on the same shape."""
+    ds = datasets("c0")
+    shape = (288, 9720)
+    e = _engine(ds, form=form, fft_shape=shape)
+    assert e.fft_shape == shape
+    s64 = _oracle_solver(oracle, ds, precision=64, fft_shape=shape)
+    e.set_plane("estimate", s64.estimate)
+    e.stage_forward()
+    for k in range(ds.workload.nexp):
+        assert rel_rms(e.plane("blur", k, as_double=True), s64.forward_blur(k)) <= tol
+    e2 = _engine(ds, form=form, fft_shape=shape)
+    e2.iterate(2)
+    s64.iterate(2)
+    assert rel_rms(e2.plane("estimate", as_double=True), s64.estimate) <= 10 * tol
+
+
 # ---------------------------------------------------------------------------- detector / update
 @pytest.mark.parametrize("background", [None, -100.0])
 def test_detector_and_adjoint_gather_bit_exact(engine_lib, oracle, datasets, background):
@@ -280,3 +300,26 @@ def test_error_negative_yeff(engine_lib, datasets, tmp_path):
     e.load(str(m), w.W, w.H, w.iw, w.ih, w.nexp)
     with pytest.raises(UpdcError, match="negative/non-finite y_eff reached solver"):
         e.setup()
+
+
+@pytest.mark.parametrize("form", ["fp32", "fp64"])
+def test_checkpoint_resume_continues_exactly(engine_lib, datasets, form, tmp_path):
+    """3 iterations, save, a fresh engine loads the state and runs 3 more:
+    identical to 6 straight iterations (estimate and FreezeMu masks), under
+    forced FreezeMu so the masks matter."""
+    from updc_b200 import _lib
+    ds = datasets("c0", background=-100.0)
+    straight = _engine(ds, form=form)
+    straight.iterate(6)
+    first = _engine(ds, form=form)
+    first.iterate(3)
+    first.save_state(tmp_path / "state.bin")
+    second = _engine(ds, form=form)
+    assert second.load_state(tmp_path / "state.bin") == 3
+    second.iterate(3)
+    np.testing.assert_array_equal(second.plane("estimate", as_double=True), straight.plane("estimate", as_double=True))
+    for k in range(ds.workload.nexp):
+        np.testing.assert_array_equal(second.plane("frozen", k), straight.plane("frozen", k))
+    other = _engine(datasets("small"), form=form)
+    with pytest.raises(_lib.UpdcError, match="does not match"):
+        other.load_state(tmp_path / "state.bin")

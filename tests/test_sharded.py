@@ -1,0 +1,118 @@
+"""Exposure-sharded solve (updc_b200/sharded.py).
+
+CPU: the exposure split, and two gloo ranks driving a small linear model of
+the same iteration (partial corrections, one all-reduce, the same update on
+both ranks) against one process holding every exposure.
+GPU: two exposure shards of one field on the same GPU, their partial
+corrections summed by the host, against the engine's own iteration.
+"""
+from __future__ import annotations
+
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+
+from updc_b200.sharded import ShardedSolver, shard_range
+
+
+def test_shard_range_covers_every_exposure_once():
+    for nexp in range(1, 13):
+        for world in range(1, nexp + 1):
+            got = [shard_range(nexp, r, world) for r in range(world)]
+            assert got[0][0] == 0 and sum(c for _, c in got) == nexp
+            assert all(a[0] + a[1] == b[0] for a, b in zip(got, got[1:]))
+            assert max(c for _, c in got) - min(c for _, c in got) <= 1
+    with pytest.raises(ValueError):
+        shard_range(3, 0, 4)
+
+
+class ToyShard:
+    """The iteration of the solver on a dense stand-in for H_k (FP64 on CPU):
+    C = sum_k H_k^T (W_k y_k / (H_k x + b_k)), D = sum_k H_k^T W_k, x *= C/D."""
+
+    def __init__(self, seed, nexp, first, count):
+        g = torch.Generator().manual_seed(seed)
+        m, n = 40, 30
+        self.H = torch.rand((nexp, m, n), generator=g, dtype=torch.float64)
+        self.W = torch.rand((nexp, m), generator=g, dtype=torch.float64) + 0.5
+        self.b = torch.rand(nexp, generator=g, dtype=torch.float64)
+        xt = torch.rand(n, generator=g, dtype=torch.float64) * 10
+        self.y = torch.einsum("kmn,n->km", self.H, xt) + self.b[:, None]
+        self.x = torch.ones(n, dtype=torch.float64)
+        self.D = torch.einsum("kmn,km->n", self.H, self.W)
+        self.first, self.count = first, count
+
+    def partial_correction(self):
+        c = torch.zeros_like(self.x)
+        for k in range(self.first, self.first + self.count):
+            mu = self.H[k] @ self.x + self.b[k]
+            c += self.H[k].T @ (self.W[k] * self.y[k] / mu)
+        return c
+
+    def broadcast_denominator(self, dist, group=None):
+        dist.broadcast(self.D, src=0, group=group)
+
+    def apply_update(self, c):
+        self.x = self.x * (c / self.D)
+        return float(self.x.sum()), int((self.x < 0).sum())
+
+
+def _gloo_rank(rank, world, port, nexp, iters, out):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        first, count = shard_range(nexp, rank, world)
+        shard = ToyShard(3, nexp, first, count)
+        recs = ShardedSolver(shard, dist).iterate(iters)
+        xs = [torch.zeros_like(shard.x) for _ in range(world)]
+        dist.all_gather(xs, shard.x)
+        if rank == 0:
+            torch.save({"x": [t.clone() for t in xs], "sums": [r["signed_sum"] for r in recs]}, out)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_match_one_process(tmp_path):
+    nexp, iters = 7, 6
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    out = tmp_path / "rank0.pt"
+    torch.multiprocessing.spawn(_gloo_rank, args=(2, port, nexp, iters, str(out)), nprocs=2, join=True)
+    got = torch.load(out)
+    ref = ToyShard(3, nexp, 0, nexp)
+    sums = [r["signed_sum"] for r in ShardedSolver(ref).iterate(iters)]
+    assert torch.equal(got["x"][0], got["x"][1])            # the estimate stays replicated
+    np.testing.assert_allclose(got["x"][0].numpy(), ref.x.numpy(), rtol=1e-12)
+    np.testing.assert_allclose(got["sums"], sums, rtol=1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form,tol", [("fp64", 1e-12), ("fp32", 1e-5)])
+def test_two_exposure_shards_match_the_whole_field(engine_lib, datasets, form, tol):
+    from updc_b200.engine import Engine
+    from updc_b200.sharded import EngineShard
+    ds = datasets("c0")
+    w = ds.workload
+
+    def engine():
+        e = Engine(form=form, use_graph=False)
+        return e.load(str(ds.manifest), w.W, w.H, w.iw, w.ih, w.nexp).setup()
+
+    whole = engine()
+    shards = [EngineShard(engine(), *shard_range(w.nexp, r, 2)) for r in range(2)]
+    for _ in range(5):
+        whole.iterate(1)
+        c = shards[0].partial_correction().clone() + shards[1].partial_correction()
+        for s in shards:
+            s.apply_update(c)
+    ref = whole.plane("estimate", as_double=True)
+    for s in shards:
+        x = s.engine.plane("estimate", as_double=True)
+        assert float(np.sqrt(np.mean((x - ref) ** 2) / np.mean(ref ** 2))) <= tol
+    np.testing.assert_array_equal(shards[0].engine.plane("estimate"), shards[1].engine.plane("estimate"))

@@ -90,6 +90,10 @@ def load() -> ctypes.CDLL:
     L.updc_batch_units.restype = c.c_size_t
     L.updc_batch_units.argtypes = [P, c.c_int]
     L.updc_batch_iterate.argtypes = [P, c.c_int, c.c_int, P, P, P, P]
+    L.updc_set_active_exposures.argtypes = [P, c.c_int, c.c_int]
+    L.updc_refresh_sensitivity.argtypes = [P]
+    L.updc_save_state.argtypes = [P, c.c_char_p, c.c_uint64]
+    L.updc_load_state.argtypes = [P, c.c_char_p, c.POINTER(c.c_uint64)]
     L.updc_link_count.restype = c.c_uint64
     L.updc_link_count.argtypes = [P, c.c_int]
     L.updc_link_encoding.argtypes = [P, c.c_int]

@@ -330,7 +330,7 @@ template <typename T> class BatchImpl final : public Batch {
         return p;
     }
     template <typename K> static void set_attr(K kern, size_t bytes) {
-        UPDC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+        raise_smem_limit(reinterpret_cast<const void *>(kern), bytes);
     }
     static size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
     size_t acc_bytes() const {

@@ -258,6 +258,32 @@ int updc_copy_plane_device(updc_engine *h, int which, int k, void *dptr, int to_
     });
 }
 
+int updc_set_active_exposures(updc_engine *h, int first, int count) {
+    return guarded([&] {
+        if (!h) throw Error(1, "null handle");
+        h->e->set_active_exposures(first, count);
+    });
+}
+int updc_refresh_sensitivity(updc_engine *h) {
+    return guarded([&] {
+        if (!h) throw Error(1, "null handle");
+        h->e->refresh_sensitivity();
+    });
+}
+
+int updc_save_state(updc_engine *h, const char *path, uint64_t iteration) {
+    return guarded([&] {
+        if (!h || !path) throw Error(1, "null argument");
+        h->e->save_state(path, iteration);
+    });
+}
+int updc_load_state(updc_engine *h, const char *path, uint64_t *iteration) {
+    return guarded([&] {
+        if (!h || !path) throw Error(1, "null argument");
+        h->e->load_state(path, iteration);
+    });
+}
+
 uint64_t updc_link_count(updc_engine *h, int k) { return h ? h->e->link_count(k) : 0; }
 int updc_link_encoding(updc_engine *h, int k) { return h ? h->e->link_encoding(k) : 0; }
 int updc_decode_links(updc_engine *h, int k, uint32_t *targets) {

@@ -5,8 +5,11 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include <map>
+#include <mutex>
 #include <stdexcept>
 #include <string>
+#include <utility>
 
 namespace updc {
 
@@ -50,6 +53,22 @@ __host__ __device__ inline uint64_t make_error_key(uint64_t stage, uint64_t inde
 }
 
 const char *error_message(uint32_t code);
+
+// Raises a kernel's dynamic shared-memory limit to at least `bytes` on the
+// current device.  The attribute belongs to the function, process-wide, so
+// it only ever grows: lowering it for one engine would make another engine's
+// launches of the same kernel (other FFT shape) fail.
+inline void raise_smem_limit(const void *func, size_t bytes) {
+    static std::mutex m;
+    static std::map<std::pair<int, const void *>, size_t> current;
+    int dev = 0;
+    UPDC_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(m);
+    size_t &c = current[{dev, func}];
+    if (bytes <= c) return;
+    UPDC_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    c = bytes;
+}
 
 // ----------------------------------------------------------------------------- complex
 template <typename T> struct cx { T x, y; };

@@ -249,9 +249,7 @@ int grid1d(size_t n, int threads = 256) {
     return (int)(g ? g : 1);
 }
 
-template <typename K> void set_smem(K kern, size_t bytes) {
-    UPDC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-}
+template <typename K> void set_smem(K kern, size_t bytes) { raise_smem_limit(reinterpret_cast<const void *>(kern), bytes); }
 
 size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
 
@@ -457,7 +455,7 @@ template <typename T> class EngineImpl final : public Engine {
         reset_iteration_state();
         launch_row_r2c_plane(estimate_, rx_, 1, 0, map_rx_);
         launch_col_forward();
-        launch_row_c2r_batched(y_, nexp_, blur_, map_y_);
+        launch_row_c2r_batched(act_y(), act_n_, blur_ + (size_t)act_k0_ * nout_, map_y_);
         UPDC_CUDA(cudaStreamSynchronize(stream_));
     }
     void stage_detector(int k, IterationRecord *rec) override {
@@ -479,7 +477,7 @@ template <typename T> class EngineImpl final : public Engine {
         (void)k;
     }
     void stage_correction() override {
-        launch_row_r2c_plane(scatter_, rs_, nexp_, nout_, map_rs_);
+        launch_row_r2c_plane(scatter_ + (size_t)act_k0_ * nout_, act_rs(), act_n_, nout_, map_rs_);
         launch_col_adjoint();
         launch_row_c2r_batched(cr_, 1, correction_, map_cr_);
         UPDC_CUDA(cudaStreamSynchronize(stream_));
@@ -494,6 +492,88 @@ template <typename T> class EngineImpl final : public Engine {
             UPDC_CUDA(cudaMemcpy(&rec->negative, d_red_neg_, 8, cudaMemcpyDeviceToHost));
         }
     }
+    // Exposures [act_k0_, act_k0_ + act_n_) take part in the iterations
+    // (all by default; an exposure shard of a multi-GPU solve otherwise).
+    int act_k0_ = 0, act_n_ = 0;
+    cx<T> *act_y() const { return y_ + (size_t)act_k0_ * ((size_t)M_ + 1) * ldh_; }
+    cx<T> *act_rs() const { return rs_ + (size_t)act_k0_ * ((size_t)M_ + 1) * ldh_; }
+    void build_exposure_maps() {
+        if (!use_tma_) return;
+        constexpr int EW = TmaElems<T>::value;
+        const uint64_t d0 = (uint64_t)ldh_ * EW;
+        const uint32_t ub = (uint32_t)row_ubox(M_);
+        make_tensor_map_3d(&map_y_, act_y(), d0, (uint64_t)M_ + 1, act_n_, row_b_ * EW, ub);
+        make_tensor_map_3d(&map_rs_, act_rs(), d0, (uint64_t)M_ + 1, act_n_, row_b_ * EW, ub);
+    }
+    void set_active_exposures(int k0, int n) override {
+        if (!setup_done_) throw Error(1, "engine is not set up");
+        if (k0 < 0 || n < 1 || k0 + n > nexp_) throw Error(1, "active exposure range out of bounds");
+        act_k0_ = k0;
+        act_n_ = n;
+        build_exposure_maps();
+        drop_loop_graphs();
+        if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+        if (graph_) cudaGraphDestroy(graph_);
+        graph_exec_ = nullptr;
+        graph_ = nullptr;
+    }
+    void refresh_sensitivity() override { finish_denominator(); }
+
+    // ------------------------------------------------------------------ checkpoint / resume
+    // State file: a 64-byte header {"UPDCSTAT", u32 version 1, u32 element
+    // bytes, u32 W, H, iw, ih, nexp, u32 0, u64 iteration, u64 0 x 2}, the
+    // estimate (W*H elements of the engine's precision) and the persistent
+    // FreezeMu masks (nexp*iw*ih bytes): everything the next iteration
+    // depends on besides the set-up products, which are rebuilt from the
+    // manifest.  Written to a temporary name and renamed into place.
+    void save_state(const std::string &path, uint64_t iteration) override {
+        if (!setup_done_) throw Error(1, "engine is not set up");
+        std::vector<T> x(nout_);
+        std::vector<uint8_t> fz(nexp_ * nin_);
+        UPDC_CUDA(cudaMemcpyAsync(x.data(), estimate_, nout_ * sizeof(T), cudaMemcpyDeviceToHost, stream_));
+        UPDC_CUDA(cudaMemcpyAsync(fz.data(), frozen_, fz.size(), cudaMemcpyDeviceToHost, stream_));
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+        unsigned char hdr[64] = {};
+        memcpy(hdr, "UPDCSTAT", 8);
+        const uint32_t f[8] = {1u, (uint32_t)sizeof(T), (uint32_t)W_, (uint32_t)H_, (uint32_t)iw_, (uint32_t)ih_,
+                               (uint32_t)nexp_, 0u};
+        memcpy(hdr + 8, f, sizeof(f));
+        memcpy(hdr + 40, &iteration, 8);
+        const std::string tmp = path + ".tmp." + std::to_string((long)getpid());
+        FILE *o = fopen(tmp.c_str(), "wb");
+        if (!o) throw Error(1, "cannot create state file: " + path);
+        const bool ok = fwrite(hdr, 1, 64, o) == 64 && fwrite(x.data(), sizeof(T), nout_, o) == nout_ &&
+                        fwrite(fz.data(), 1, fz.size(), o) == fz.size();
+        if (fclose(o) || !ok || rename(tmp.c_str(), path.c_str())) {
+            unlink(tmp.c_str());
+            throw Error(1, "state file write failed: " + path);
+        }
+    }
+    void load_state(const std::string &path, uint64_t *iteration) override {
+        if (!setup_done_) throw Error(1, "engine is not set up");
+        FILE *in = fopen(path.c_str(), "rb");
+        if (!in) throw Error(1, "cannot open state file: " + path);
+        unsigned char hdr[64];
+        uint32_t f[8];
+        std::vector<T> x(nout_);
+        std::vector<uint8_t> fz(nexp_ * nin_);
+        bool ok = fread(hdr, 1, 64, in) == 64 && memcmp(hdr, "UPDCSTAT", 8) == 0;
+        if (ok) {
+            memcpy(f, hdr + 8, sizeof(f));
+            ok = f[0] == 1u && f[1] == sizeof(T) && f[2] == (uint32_t)W_ && f[3] == (uint32_t)H_ &&
+                 f[4] == (uint32_t)iw_ && f[5] == (uint32_t)ih_ && f[6] == (uint32_t)nexp_;
+        }
+        ok = ok && fread(x.data(), sizeof(T), nout_, in) == nout_ && fread(fz.data(), 1, fz.size(), in) == fz.size();
+        char extra;
+        ok = ok && fread(&extra, 1, 1, in) == 0;
+        fclose(in);
+        if (!ok) throw Error(1, "state file does not match this field and precision: " + path);
+        if (iteration) memcpy(iteration, hdr + 40, 8);
+        UPDC_CUDA(cudaMemcpyAsync(estimate_, x.data(), nout_ * sizeof(T), cudaMemcpyHostToDevice, stream_));
+        UPDC_CUDA(cudaMemcpyAsync(frozen_, fz.data(), fz.size(), cudaMemcpyHostToDevice, stream_));
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+    }
+
     FieldView field_view() const override {
         if (!setup_done_) throw Error(1, "engine is not set up");
         FieldView v;
@@ -593,8 +673,8 @@ template <typename T> class EngineImpl final : public Engine {
         // X = FFT2(pad(x)), A = FFT2(pad(S^T r_k)), both u-major (M+1) x FH
         launch_row_r2c_plane(estimate_, rx_, 1, 0, map_rx_);
         launch_col_fft<false>(rx_, ldh_, H_, xs, FH_, FH_);
-        launch_row_r2c_plane(scatter_ + (size_t)k * nout_, rs_, 1, 0, map_rs_);
-        launch_col_fft<false>(rs_, ldh_, H_, as, FH_, FH_);
+        launch_row_r2c_plane(scatter_ + (size_t)k * nout_, act_rs(), 1, 0, map_rs_);
+        launch_col_fft<false>(act_rs(), ldh_, H_, as, FH_, FH_);
         // correlation c = IFFT2(A conj(X)) / nf, kept on the PSF window
         k_mul_conj<T><<<grid1d(ns), 256, 0, stream_>>>(as, xs, ns);
         launch_col_fft<true>(as, FH_, FH_, xs, FH_, FH_);
@@ -1108,10 +1188,21 @@ template <typename T> class EngineImpl final : public Engine {
             const uint32_t ub = (uint32_t)row_ubox(M_);
             make_tensor_map_3d(&map_rx_, rx_, d0, nu, 1, row_b_ * EW, ub);
             make_tensor_map_3d(&map_cr_, cr_, d0, nu, 1, row_b_ * EW, ub);
-            make_tensor_map_3d(&map_y_, y_, d0, nu, nexp_, row_b_ * EW, ub);
-            make_tensor_map_3d(&map_rs_, rs_, d0, nu, nexp_, row_b_ * EW, ub);
         }
+        act_k0_ = 0;
+        act_n_ = nexp_;
+        build_exposure_maps();
         configure_kernels();
+        // the adjoint's accumulator plane, when it does not fit shared memory,
+        // is allocated here: iterations are captured into graphs, where no
+        // allocation may happen
+        if constexpr (sizeof(T) == 4) {
+            if (opt_.form == FORM_FP32) ensure_adj_aux<AccF64>();
+            else if (opt_.form == FORM_FP32_KAHAN) ensure_adj_aux<AccKahan>();
+            else ensure_adj_aux<AccPlain<T>>();
+        } else {
+            ensure_adj_aux<AccPlain<T>>();
+        }
     }
 
     // ------------------------------------------------------------------ kernel configuration
@@ -1180,10 +1271,13 @@ template <typename T> class EngineImpl final : public Engine {
         const size_t nu = (size_t)M_ + 1;
         const size_t ks = nu * FH_, ys = nu * ldh_;
         if (FH_ <= Caps<T>::COL_S)
-            k_col_forward<T, NT, Caps<T>::COL_S><<<(unsigned)nu, NT, fwd_smem(), stream_>>>(plan_h_, rx_, ldh_, H_, khat_, ks, nexp_, y_, ldh_, ys, H_, (int)nu, aux_fwd_);
+            k_col_forward<T, NT, Caps<T>::COL_S><<<(unsigned)nu, NT, fwd_smem(), stream_>>>(plan_h_, rx_, ldh_, H_, khat_ + act_k0_ * ks, ks, act_n_, act_y(), ldh_, ys, H_, (int)nu, aux_fwd_);
         else
-            k_col_forward<T, NT, Caps<T>::COL_L><<<(unsigned)nu, NT, fwd_smem(), stream_>>>(plan_h_, rx_, ldh_, H_, khat_, ks, nexp_, y_, ldh_, ys, H_, (int)nu, aux_fwd_);
+            k_col_forward<T, NT, Caps<T>::COL_L><<<(unsigned)nu, NT, fwd_smem(), stream_>>>(plan_h_, rx_, ldh_, H_, khat_ + act_k0_ * ks, ks, act_n_, act_y(), ldh_, ys, H_, (int)nu, aux_fwd_);
         UPDC_CUDA(cudaGetLastError());
+    }
+    template <class Acc> void ensure_adj_aux() {
+        if (adj_aux<Acc>() && !aux_adj_) aux_adj_ = alloc<typename Acc::S>(((size_t)M_ + 1) * FH_);
     }
     template <class Acc> void launch_col_adjoint_t(const cx<T> *khat) {
         const size_t nu = (size_t)M_ + 1;
@@ -1194,9 +1288,9 @@ template <typename T> class EngineImpl final : public Engine {
         }
         const size_t s = adj_smem<Acc>();
         if (FH_ <= Caps<T>::COL_S)
-            k_col_adjoint<T, Acc, NtAdj<T>::value, Caps<T>::COL_S><<<(unsigned)nu, NtAdj<T>::value, s, stream_>>>(plan_h_, rs_, ldh_, nu * ldh_, H_, khat, nu * FH_, nexp_, cr_, ldh_, H_, aux);
+            k_col_adjoint<T, Acc, NtAdj<T>::value, Caps<T>::COL_S><<<(unsigned)nu, NtAdj<T>::value, s, stream_>>>(plan_h_, act_rs(), ldh_, nu * ldh_, H_, khat + act_k0_ * nu * FH_, nu * FH_, act_n_, cr_, ldh_, H_, aux);
         else
-            k_col_adjoint<T, Acc, NtAdj<T>::value, Caps<T>::COL_L><<<(unsigned)nu, NtAdj<T>::value, s, stream_>>>(plan_h_, rs_, ldh_, nu * ldh_, H_, khat, nu * FH_, nexp_, cr_, ldh_, H_, aux);
+            k_col_adjoint<T, Acc, NtAdj<T>::value, Caps<T>::COL_L><<<(unsigned)nu, NtAdj<T>::value, s, stream_>>>(plan_h_, act_rs(), ldh_, nu * ldh_, H_, khat + act_k0_ * nu * FH_, nu * FH_, act_n_, cr_, ldh_, H_, aux);
         UPDC_CUDA(cudaGetLastError());
     }
     void launch_col_adjoint() {
@@ -1225,14 +1319,20 @@ template <typename T> class EngineImpl final : public Engine {
         return (T)(1.0 / (double)((size_t)FW_ * FH_));
     }
     void launch_detector() {
-        dim3 grid((unsigned)std::min<size_t>(ceil_div(nin_, 256), 148 * 8), (unsigned)nexp_);
-        if (comp_mu_) k_detector<T, true><<<grid, 256, 0, stream_>>>(d_exps_, nin_, nout_, blur_, wr_, d_stats_, d_err_);
-        else k_detector<T, false><<<grid, 256, 0, stream_>>>(d_exps_, nin_, nout_, blur_, wr_, d_stats_, d_err_);
+        dim3 grid((unsigned)std::min<size_t>(ceil_div(nin_, 256), 148 * 8), (unsigned)act_n_);
+        const size_t k0 = act_k0_;
+        if (comp_mu_)
+            k_detector<T, true><<<grid, 256, 0, stream_>>>(d_exps_ + k0, nin_, nout_, blur_ + k0 * nout_, wr_ + k0 * nin_,
+                                                            d_stats_ + k0, d_err_);
+        else
+            k_detector<T, false><<<grid, 256, 0, stream_>>>(d_exps_ + k0, nin_, nout_, blur_ + k0 * nout_, wr_ + k0 * nin_,
+                                                             d_stats_ + k0, d_err_);
         UPDC_CUDA(cudaGetLastError());
     }
     void launch_scatter(const T *vals, T *out) {
-        dim3 grid((unsigned)std::min<size_t>(ceil_div(nout_, 256), 148 * 8), (unsigned)nexp_);
-        k_scatter_t<T, T, T><<<grid, 256, 0, stream_>>>(d_exps_, nin_, nout_, vals, 0, out);
+        dim3 grid((unsigned)std::min<size_t>(ceil_div(nout_, 256), 148 * 8), (unsigned)act_n_);
+        const size_t k0 = act_k0_;
+        k_scatter_t<T, T, T><<<grid, 256, 0, stream_>>>(d_exps_ + k0, nin_, nout_, vals + k0 * nin_, 0, out + k0 * nout_);
         UPDC_CUDA(cudaGetLastError());
     }
     void launch_update() {
@@ -1265,13 +1365,13 @@ template <typename T> class EngineImpl final : public Engine {
         if (timed) UPDC_CUDA(cudaEventRecord(ev[1], stream_));
         launch_col_forward();                                               // y pass + OTF + inverse y pass
         if (timed) UPDC_CUDA(cudaEventRecord(ev[2], stream_));
-        launch_row_c2r_batched(y_, nexp_, blur_, map_y_);                           // inverse x pass + crop
+        launch_row_c2r_batched(act_y(), act_n_, blur_ + (size_t)act_k0_ * nout_, map_y_);  // inverse x pass + crop
         if (timed) UPDC_CUDA(cudaEventRecord(ev[3], stream_));
         launch_detector();                                                  // gather / FreezeMu / ratio
         if (timed) UPDC_CUDA(cudaEventRecord(ev[4], stream_));
         launch_scatter(wr_, scatter_);                                      // S^T (transposed gather)
         if (timed) UPDC_CUDA(cudaEventRecord(ev[5], stream_));
-        launch_row_r2c_plane(scatter_, rs_, nexp_, nout_, map_rs_);  // scatter R2C, x pass
+        launch_row_r2c_plane(scatter_ + (size_t)act_k0_ * nout_, act_rs(), act_n_, nout_, map_rs_);  // scatter R2C, x pass
         if (timed) UPDC_CUDA(cudaEventRecord(ev[6], stream_));
         launch_col_adjoint();                                               // y pass, conj-OTF sum, inverse y
         launch_row_c2r_batched(cr_, 1, correction_, map_cr_);                        // inverse x pass + crop
@@ -1340,7 +1440,15 @@ template <typename T> class EngineImpl final : public Engine {
         reset_iteration_state();
         UPDC_CUDA(cudaStreamSynchronize(stream_));
         UPDC_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-        enqueue_iteration(false);
+        try {
+            enqueue_iteration(false);
+        } catch (...) {
+            // end the capture, or every later call of this thread fails
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(stream_, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
         UPDC_CUDA(cudaStreamEndCapture(stream_, &graph_));
         UPDC_CUDA(cudaGraphInstantiate(&graph_exec_, graph_, 0));
     }

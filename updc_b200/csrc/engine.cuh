@@ -111,6 +111,16 @@ class Engine {
     // Plane <-> caller device memory (to_engine = 1 writes the plane), on the
     // engine's stream after `stream` (0: legacy default) has reached this call.
     virtual void copy_plane_device(int which, int k, void *dptr, int to_engine, int as_double, cudaStream_t stream) = 0;
+    // Iterate only exposures [k0, k0 + n) (an exposure shard of a multi-GPU
+    // solve: every other setup product stays that of the whole field).
+    virtual void set_active_exposures(int k0, int n) = 0;
+    // Recompute max_sensitivity from the denominator plane (after it was
+    // replaced, e.g. by a sum over shards).
+    virtual void refresh_sensitivity() = 0;
+    // Checkpoint / resume: the estimate and the FreezeMu masks with the
+    // iteration count they belong to.
+    virtual void save_state(const std::string &path, uint64_t iteration) = 0;
+    virtual void load_state(const std::string &path, uint64_t *iteration) = 0;
     // Device-side view of the set-up field for the batched launches (batch.cu).
     virtual struct FieldView field_view() const = 0;
 };

@@ -206,6 +206,27 @@ class Engine:
         check(self._L.updc_stage_update(self._h, ctypes.byref(s), ctypes.byref(n)))
         return s.value, int(n.value)
 
+    # ------------------------------------------------------------------ checkpoint / resume
+    def save_state(self, path, iteration: Optional[int] = None) -> None:
+        """Write the estimate and the FreezeMu masks (with the iteration count)."""
+        check(self._L.updc_save_state(self._h, str(path).encode(),
+                                      self.iterations_done if iteration is None else iteration))
+
+    def load_state(self, path) -> int:
+        """Restore a state written by save_state on the same field and form;
+        returns its iteration count (also set as iterations_done)."""
+        it = ctypes.c_uint64()
+        check(self._L.updc_load_state(self._h, str(path).encode(), ctypes.byref(it)))
+        self.iterations_done = int(it.value)
+        return self.iterations_done
+
+    # ------------------------------------------------------------------ exposure shards
+    def set_active_exposures(self, first: int, count: int) -> None:
+        check(self._L.updc_set_active_exposures(self._h, first, count))
+
+    def refresh_sensitivity(self) -> None:
+        check(self._L.updc_refresh_sensitivity(self._h))
+
     # ------------------------------------------------------------------ differentiable model
     def set_exposure_offsets(self, exposure: int, background: float, pedestal: float) -> None:
         check(self._L.updc_set_exposure_offsets(self._h, exposure, float(background), float(pedestal)))

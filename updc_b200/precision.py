@@ -40,10 +40,13 @@ def run_forms(manifest: str, W: int, H: int, iw: int, ih: int, nexp: int, iterat
     """Returns {form: [per-iteration record]} with errors against the FP64 form."""
     out: Dict[str, list] = {}
     for form in forms:
-        ref = Engine(form="fp64", device=device)
-        ref.load(manifest, W, H, iw, ih, nexp).setup()
+        # the FP32 form first: its one-time FP64 denominator needs transient
+        # memory that must not coincide with the FP64 engine's planes (c4
+        # holds ~150 GB with both engines alive)
         eng = Engine(form=form, device=device)
         eng.load(manifest, W, H, iw, ih, nexp).setup()
+        ref = Engine(form="fp64", device=device)
+        ref.load(manifest, W, H, iw, ih, nexp).setup()
         recs = []
         for it in range(1, iterations + 1):
             sr = ref.iterate(1)[0]
@@ -89,6 +92,11 @@ def main(argv=None) -> int:
         t0 = time.time()
         ds = synth.generate(w.name, d)
         gen = time.time() - t0
+        try:
+            import torch
+            torch.cuda.empty_cache()         # the generator's device buffers
+        except ImportError:
+            pass
         res = run_forms(str(ds.manifest), w.W, w.H, w.iw, w.ih, w.nexp, its, a.forms.split(","))
     s = summary(res)
     print(json.dumps({"workload": a.workload, "iterations": its, "generate_s": round(gen, 1), "forms": s}))
