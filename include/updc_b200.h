@@ -222,6 +222,16 @@ size_t updc_batch_units(updc_batch *b, int stage);
 int updc_batch_iterate(updc_batch *b, int n, int check_each, double *seconds, double *signed_sum, uint64_t *negative,
                        uint64_t *total_frozen);
 
+/* PSF projection (psf_projector.c:82-172) on the GPU: input PSF (raw f32,
+ * width x height) and its (width+1) x (height+1) mapped corner offsets (raw
+ * f64 x,y pairs) -> projected PSF (raw f32, out_width x out_height, the
+ * symmetric extent of the mapped corners), bit-identical to the reference
+ * projector.  Returns 0, 1 with the reference's message, or 2 when the
+ * projection is not flux-conserving (|rel| > 5e-5; the sums are filled). */
+int updc_psf_project_file(const char *input, int width, int height, const char *vertices, const char *output,
+                          int *out_width, int *out_height, double *input_sum, double *output_sum, uint64_t *overlaps,
+                          char *message, size_t capacity);
+
 /* Geometry (overlap.c:72-116) and the known-answer self-test (updc_core.c:1545-1564). */
 float updc_polygon_area(const double *xy, int count);
 float updc_overlap_area(const double *quad8, int x, int y);

@@ -19,6 +19,7 @@ HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "_build" / "liboracle.so"
 SHIM_PATH = HERE / "_build" / "libfftw_shim.so"
 REF_BINARY = HERE / "_ref" / "updc_jwst_c"
+REF_PROJECTOR = HERE / "_ref" / "updc_psf_projector"
 REFERENCE_SOURCES = Path("/root/reference/updc/c_core")
 
 _lib = None

@@ -21,13 +21,14 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libupdc_b200.so"
 EXE = PKG / "bin" / "updc_jwst_c"
+PROJECTOR = PKG / "bin" / "updc_psf_projector"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
               "-Xcompiler", "-Wall", "-I", str(ROOT / "include")]
 # geometry must not contract multiply-adds (bit-exact LinkMaps)
-PER_FILE = {"linkmap.cu": ["-fmad=false"]}
-SOURCES = ["linkmap.cu", "engine.cu", "capi.cu", "noalloc.cu", "batch.cu"]
+PER_FILE = {"linkmap.cu": ["-fmad=false"], "projector.cu": ["-fmad=false"]}
+SOURCES = ["linkmap.cu", "engine.cu", "capi.cu", "noalloc.cu", "batch.cu", "projector.cu"]
 HEADERS = ["common.cuh", "fft.cuh", "kernels.cuh", "pointwise.cuh", "engine.cuh", "geometry.cuh", "linkmap.cuh",
            "tma.cuh", "nll.cuh"]
 
@@ -71,13 +72,13 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode:
             raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
-    main_src = CSRC / "updc_jwst_c.c"
-    if force or _stale(EXE, [LIB, main_src]):
-        cmd = ["gcc", "-O2", "-std=c11", "-Wall", "-o", str(EXE), str(main_src), f"-L{PKG}", "-lupdc_b200",
-               f"-Wl,-rpath,$ORIGIN/.."]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode:
-            raise RuntimeError("executable link failed:\n" + r.stdout + r.stderr)
+    for exe, main_src in ((EXE, CSRC / "updc_jwst_c.c"), (PROJECTOR, CSRC / "updc_psf_projector.c")):
+        if force or _stale(exe, [LIB, main_src]):
+            cmd = ["gcc", "-O2", "-std=gnu11", "-Wall", "-o", str(exe), str(main_src), f"-L{PKG}", "-lupdc_b200",
+                   f"-Wl,-rpath,$ORIGIN/.."]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode:
+                raise RuntimeError("executable link failed:\n" + r.stdout + r.stderr)
     return LIB
 
 

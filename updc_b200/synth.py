@@ -366,3 +366,31 @@ def generate_batch(directory: os.PathLike, n_fields: int = 64, seed: int = 2,
     d = Path(directory)
     return [generate(w, d / w.name, use_torch=False) for w in batch_workloads(n_fields, seed, iterations)]
 
+
+# ----------------------------------------------------------------------------- PSF projection cases
+def psf_projection_case(directory: os.PathLike, name: str, size: int, oversample: int, seed: int,
+                        distortion: float = 1.0e-4):
+    """An oversampled Gaussian+Moffat PSF (size x size, odd) and the target
+    offsets of its pixel corners: a detector-pixel offset (i - size/2) /
+    oversample mapped by 2 x rotation x scale x shear plus a quadratic
+    distortion, centred on the PSF centre (the layout of _engine.py:470-521's
+    vertex files).  Writes <name>.f32 and <name>.vertices.bin; returns their
+    paths."""
+    rng = np.random.default_rng(seed)
+    d = Path(directory)
+    d.mkdir(parents=True, exist_ok=True)
+    psf = gauss_moffat_psf(size, sigma=float(rng.uniform(1.0, 2.5)))
+    g = (np.arange(size + 1, dtype=np.float64) - size / 2.0) / float(oversample)
+    xx, yy = np.meshgrid(g, g)
+    th = np.deg2rad(rng.uniform(-30.0, 30.0))
+    s = 2.0 * rng.uniform(0.98, 1.02)
+    sh = rng.uniform(-0.01, 0.01)
+    A = s * np.array([[np.cos(th), -np.sin(th)], [np.sin(th), np.cos(th)]]) @ np.array([[1.0, sh], [0.0, 1.0]])
+    px = A[0, 0] * xx + A[0, 1] * yy + distortion * (xx * xx - yy * yy)
+    py = A[1, 0] * xx + A[1, 1] * yy + distortion * 2.0 * xx * yy
+    f_psf = d / f"{name}.f32"
+    f_vert = d / f"{name}.vertices.bin"
+    psf.astype("<f4").tofile(f_psf)
+    np.stack((px, py), axis=-1).astype("<f8").tofile(f_vert)
+    return f_psf, f_vert
+
