@@ -233,6 +233,7 @@ namespace {
 
 constexpr int NT = SPEC_NT;
 template <typename T> using NtAdj = SpecNtAdj<T>;
+template <typename T> using ColNt = SpecColNt<T>;
 template <typename T> using Caps = SpecCaps<T>;
 constexpr size_t SMEM_LIMIT = SPEC_SMEM_LIMIT;
 
@@ -589,15 +590,13 @@ template <typename T> class EngineImpl final : public Engine {
         v.post = post_;
         v.estimate = estimate_, v.den = den_, v.correction = correction_, v.blur = blur_, v.scatter = scatter_, v.wr = wr_;
         v.rx = rx_, v.y = y_, v.rs = rs_, v.cr = cr_, v.khat = khat_;
-        bool adj = false;
-        if constexpr (sizeof(T) == 4) {
-            if (opt_.form == FORM_FP32) adj = adj_aux<AccF64>();
-            else if (opt_.form == FORM_FP32_KAHAN) adj = adj_aux<AccKahan>();
-            else adj = adj_aux<AccPlain<T>>();
-        } else {
-            adj = adj_aux<AccPlain<T>>();
-        }
-        v.needs_aux = aux_fwd_ != nullptr || adj || FH_ > Caps<T>::COL_S;
+        // the batched column kernels keep X-hat and the accumulator in shared memory
+        const size_t fb = fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift);
+        size_t accb = sizeof(cx<T>);
+        if (sizeof(T) == 4 && opt_.form == FORM_FP32) accb = sizeof(AccF64::S);
+        if (sizeof(T) == 4 && opt_.form == FORM_FP32_KAHAN) accb = sizeof(AccKahan::S);
+        v.needs_aux = FH_ > Caps<T>::COL_S || fb + align16((size_t)FH_ * sizeof(cx<T>)) > SMEM_LIMIT ||
+                      fb + align16((size_t)FH_ * accb) > SMEM_LIMIT;
         v.exps = d_exps_;
         v.stats = d_stats_;
         v.err = d_err_;
@@ -993,22 +992,23 @@ template <typename T> class EngineImpl final : public Engine {
         for (const auto &rad : split_candidates(FH)) {
             FftPlan plan;
             auto tab = fft_make_table<T>(FH, rad, plan);
-            plan.pad_shift = fft_choose_padding(plan, NT, Caps<T>::COL_S, 1);
+            plan.pad_shift = fft_choose_padding(plan, ColNt<T>::value, Caps<T>::COL_S, 1);
             const size_t smem = fft_buf_bytes(FH, sizeof(cx<T>), plan.pad_shift);
             if (smem > SMEM_LIMIT) continue;
             cx<T> *dtab = dalloc<cx<T>>(tab.size(), nullptr);
             UPDC_CUDA(cudaMemcpy(dtab, tab.data(), tab.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
             plan.tw = dtab;
             float ms;
+            constexpr int CNT = ColNt<T>::value;
             if (FH <= Caps<T>::COL_S) {
-                set_smem(k_col_fft<T, NT, Caps<T>::COL_S, false>, smem);
+                set_smem(k_col_fft<T, CNT, Caps<T>::COL_S, false>, smem);
                 ms = time_launch([&] {
-                    k_col_fft<T, NT, Caps<T>::COL_S, false><<<(unsigned)nc, NT, smem, stream_>>>(plan, in, H_, H_, out, FH, FH);
+                    k_col_fft<T, CNT, Caps<T>::COL_S, false><<<(unsigned)nc, CNT, smem, stream_>>>(plan, in, H_, H_, out, FH, FH);
                 });
             } else {
-                set_smem(k_col_fft<T, NT, Caps<T>::COL_L, false>, smem);
+                set_smem(k_col_fft<T, CNT, Caps<T>::COL_L, false>, smem);
                 ms = time_launch([&] {
-                    k_col_fft<T, NT, Caps<T>::COL_L, false><<<(unsigned)nc, NT, smem, stream_>>>(plan, in, H_, H_, out, FH, FH);
+                    k_col_fft<T, CNT, Caps<T>::COL_L, false><<<(unsigned)nc, CNT, smem, stream_>>>(plan, in, H_, H_, out, FH, FH);
                 });
             }
             ++*timed;
@@ -1127,7 +1127,7 @@ template <typename T> class EngineImpl final : public Engine {
         auto tm = fft_make_table<T>(M_, c.row_radices, plan_m_);
         auto th = fft_make_table<T>(FH_, c.col_radices, plan_h_);
         plan_m_.pad_shift = fft_choose_padding(plan_m_, NT, Caps<T>::ROW, std::max(1, std::min(2, Caps<T>::ROW / M_)));
-        plan_h_.pad_shift = fft_choose_padding(plan_h_, NT, Caps<T>::COL_S, 1);
+        plan_h_.pad_shift = fft_choose_padding(plan_h_, ColNt<T>::value, Caps<T>::COL_S, 1);
         cx<T> *dm = alloc<cx<T>>(tm.size()), *dh = alloc<cx<T>>(th.size());
         UPDC_CUDA(cudaMemcpy(dm, tm.data(), tm.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
         UPDC_CUDA(cudaMemcpy(dh, th.data(), th.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
@@ -1171,7 +1171,8 @@ template <typename T> class EngineImpl final : public Engine {
         d_part_neg_ = alloc<unsigned long long>(upd_grid_);
         d_red_sum_ = alloc<double>(1);
         d_red_neg_ = alloc<unsigned long long>(1);
-        if (fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift) + align16((size_t)FH_ * sizeof(cx<T>)) > SMEM_LIMIT) aux_fwd_ = alloc<cx<T>>(nu * FH_);
+        if (cols_in_global() || fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift) + align16((size_t)FH_ * sizeof(cx<T>)) > SMEM_LIMIT)
+            aux_fwd_ = alloc<cx<T>>(nu * FH_);
         links_.assign(nexp_, DevLinkMap());
         // rows per row-transform block; the TMA path needs an even number of
         // 8-byte elements per row tile (16-byte box rows and coordinates)
@@ -1217,12 +1218,17 @@ template <typename T> class EngineImpl final : public Engine {
     size_t fwd_smem() const {
         return fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift) + (aux_fwd_ ? 0 : align16(FH_ * sizeof(cx<T>)));
     }
+    // FP32 column kernels keep X-hat and the adjoint accumulator of their
+    // column in a global scratch (L2-resident: ~50 MB for all resident
+    // blocks) so that three blocks fit an SM.
+    static constexpr bool cols_in_global() { return sizeof(T) == 4; }
     template <class Acc> size_t adj_smem() const {
         const size_t b = fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift) + align16(FH_ * sizeof(typename Acc::S));
-        return b > SMEM_LIMIT ? fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift) : b;
+        return adj_aux<Acc>() ? fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift) : b;
     }
     template <class Acc> bool adj_aux() const {
-        return fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift) + align16(FH_ * sizeof(typename Acc::S)) > SMEM_LIMIT;
+        return cols_in_global() ||
+               fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift) + align16(FH_ * sizeof(typename Acc::S)) > SMEM_LIMIT;
     }
 
     void configure_kernels() {
@@ -1232,8 +1238,8 @@ template <typename T> class EngineImpl final : public Engine {
         set_smem(k_row_c2r<T, NT, Caps<T>::ROW, PlaneStore<T>, true>, rs);
         set_smem(k_row_c2r<T, NT, Caps<T>::ROW, PlaneStore<T>, false>, rs);
         const size_t fs = fwd_smem();
-        set_smem(k_col_forward<T, NT, Caps<T>::COL_S>, fs);
-        set_smem(k_col_forward<T, NT, Caps<T>::COL_L>, fs);
+        set_smem(k_col_forward<T, ColNt<T>::value, Caps<T>::COL_S>, fs);
+        set_smem(k_col_forward<T, ColNt<T>::value, Caps<T>::COL_L>, fs);
         set_smem(k_col_fft<T, NT, Caps<T>::COL_S, false>, fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift));
         set_smem(k_col_fft<T, NT, Caps<T>::COL_L, false>, fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift));
         configure_adjoint<AccPlain<T>>();
@@ -1246,8 +1252,8 @@ template <typename T> class EngineImpl final : public Engine {
         if constexpr (sizeof(typename Acc::S) > 0) {
             if constexpr (std::is_same<Acc, AccPlain<T>>::value || sizeof(T) == 4) {
                 const size_t s = adj_smem<Acc>();
-                set_smem(k_col_adjoint<T, Acc, NtAdj<T>::value, Caps<T>::COL_S>, s);
-                set_smem(k_col_adjoint<T, Acc, NtAdj<T>::value, Caps<T>::COL_L>, s);
+                set_smem(k_col_adjoint<T, Acc, ColNt<T>::value, Caps<T>::COL_S>, s);
+                set_smem(k_col_adjoint<T, Acc, ColNt<T>::value, Caps<T>::COL_L>, s);
             }
         }
     }
@@ -1271,9 +1277,9 @@ template <typename T> class EngineImpl final : public Engine {
         const size_t nu = (size_t)M_ + 1;
         const size_t ks = nu * FH_, ys = nu * ldh_;
         if (FH_ <= Caps<T>::COL_S)
-            k_col_forward<T, NT, Caps<T>::COL_S><<<(unsigned)nu, NT, fwd_smem(), stream_>>>(plan_h_, rx_, ldh_, H_, khat_ + act_k0_ * ks, ks, act_n_, act_y(), ldh_, ys, H_, (int)nu, aux_fwd_);
+            k_col_forward<T, ColNt<T>::value, Caps<T>::COL_S><<<(unsigned)nu, ColNt<T>::value, fwd_smem(), stream_>>>(plan_h_, rx_, ldh_, H_, khat_ + act_k0_ * ks, ks, act_n_, act_y(), ldh_, ys, H_, (int)nu, aux_fwd_);
         else
-            k_col_forward<T, NT, Caps<T>::COL_L><<<(unsigned)nu, NT, fwd_smem(), stream_>>>(plan_h_, rx_, ldh_, H_, khat_ + act_k0_ * ks, ks, act_n_, act_y(), ldh_, ys, H_, (int)nu, aux_fwd_);
+            k_col_forward<T, ColNt<T>::value, Caps<T>::COL_L><<<(unsigned)nu, ColNt<T>::value, fwd_smem(), stream_>>>(plan_h_, rx_, ldh_, H_, khat_ + act_k0_ * ks, ks, act_n_, act_y(), ldh_, ys, H_, (int)nu, aux_fwd_);
         UPDC_CUDA(cudaGetLastError());
     }
     template <class Acc> void ensure_adj_aux() {
@@ -1288,9 +1294,9 @@ template <typename T> class EngineImpl final : public Engine {
         }
         const size_t s = adj_smem<Acc>();
         if (FH_ <= Caps<T>::COL_S)
-            k_col_adjoint<T, Acc, NtAdj<T>::value, Caps<T>::COL_S><<<(unsigned)nu, NtAdj<T>::value, s, stream_>>>(plan_h_, act_rs(), ldh_, nu * ldh_, H_, khat + act_k0_ * nu * FH_, nu * FH_, act_n_, cr_, ldh_, H_, aux);
+            k_col_adjoint<T, Acc, ColNt<T>::value, Caps<T>::COL_S><<<(unsigned)nu, ColNt<T>::value, s, stream_>>>(plan_h_, act_rs(), ldh_, nu * ldh_, H_, khat + act_k0_ * nu * FH_, nu * FH_, act_n_, cr_, ldh_, H_, aux);
         else
-            k_col_adjoint<T, Acc, NtAdj<T>::value, Caps<T>::COL_L><<<(unsigned)nu, NtAdj<T>::value, s, stream_>>>(plan_h_, act_rs(), ldh_, nu * ldh_, H_, khat + act_k0_ * nu * FH_, nu * FH_, act_n_, cr_, ldh_, H_, aux);
+            k_col_adjoint<T, Acc, ColNt<T>::value, Caps<T>::COL_L><<<(unsigned)nu, ColNt<T>::value, s, stream_>>>(plan_h_, act_rs(), ldh_, nu * ldh_, H_, khat + act_k0_ * nu * FH_, nu * FH_, act_n_, cr_, ldh_, H_, aux);
         UPDC_CUDA(cudaGetLastError());
     }
     void launch_col_adjoint() {
