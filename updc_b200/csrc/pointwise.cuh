@@ -208,8 +208,10 @@ __device__ __forceinline__ void detector_tiles(const ExpDesc<T> &e, int k, size_
     }
 }
 
+// Four 256-thread blocks per SM (64 registers; measured 5% faster than three
+// blocks at 80 registers on B200).
 template <typename T, bool COMP>
-__global__ void __launch_bounds__(DET_WARPS * 32) k_detector(const ExpDesc<T> *__restrict__ exps, size_t nin, size_t nout,
+__global__ void __launch_bounds__(DET_WARPS * 32, 4) k_detector(const ExpDesc<T> *__restrict__ exps, size_t nin, size_t nout,
                                                            const T *__restrict__ blur_all, T *__restrict__ wr_all,
                                                            ExpStats *__restrict__ stats, unsigned long long *__restrict__ err) {
     const int k = blockIdx.y;
