@@ -130,8 +130,8 @@ def stage_bytes(w, fw, fh, links, tlinks, dtype_bytes=4):
 # FFT 3584^2): the kernels' traffic grows in proportion to the columns, rows
 # and exposures they process, so this ratio carries a capture of the small
 # case to the benchmark's workload.
-TRAFFIC_RATIO_C3 = {"estimate_x_pass": 18.4 / 46.2, "forward_y_passes": 322.0 / 352.5, "forward_x_pass": 155.2 / 184.6,
-                    "scatter_x_pass": 134.5 / 184.6, "adjoint_y_x_passes": (349.1 + 29.6) / (352.5 + 46.2)}
+TRAFFIC_RATIO_C3 = {"estimate_x_pass": 17.9 / 46.2, "forward_y_passes": 366.4 / 352.5, "forward_x_pass": 155.7 / 184.6,
+                    "scatter_x_pass": 130.8 / 184.6, "adjoint_y_x_passes": (426.8 + 29.0) / (352.5 + 46.2)}
 
 STAGES = ["estimate_x_pass", "forward_y_passes", "forward_x_pass", "detector", "adjoint_gather",
           "scatter_x_pass", "adjoint_y_x_passes", "update"]
