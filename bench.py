@@ -16,6 +16,8 @@ rank computes the partial correction of its exposures, one NCCL all-reduce
 sums them and every rank applies the same update (strong scaling; --replicas
 runs N independent copies instead).  ``--workload c2`` runs 64 batched
 cutout fields, every stage one persistent launch over all fields.
+``--workload pre`` times the per-exposure weight preprocessing (sigma-clipped
+sky, weights, pedestals, WHT; updc/_engine.py:287-408) of the c1 exposures.
 """
 from __future__ import annotations
 
@@ -125,6 +127,33 @@ def stage_bytes(w, fw, fh, links, tlinks, dtype_bytes=4):
     }
 
 
+def model_bytes(w, fw, fh, links, dtype_bytes=4):
+    """Algorithmic bytes of each stage under the path's stated model: every
+    2-D FFT is two passes, each reading and writing the full FH x (FW/2+1)
+    spectrum Sc (so 2 Sc per pass), an OTF read is Sc, the cross-exposure
+    accumulator is read and written once per exposure (2 Sc), the detector
+    loop reads its LinkMap, SCI, W, the mask and blur_k, and the scatter plane
+    is written once (St).  The engine itself moves fewer bytes (the zero
+    padding of the passes is never stored, the accumulator stays on chip or in
+    L2): `stage_bytes` is that tighter count."""
+    N, nin, nout = w.nexp, w.iw * w.ih, w.W * w.H
+    c, r = 2 * dtype_bytes, dtype_bytes
+    Sc = (fw // 2 + 1) * fh * c
+    St, Sd = nout * r, nin * r
+    link_bytes = sum(4 * (nin + 1) + (4 * nin + 2 * L + (2 * L) % 4 if enc == 2 else 4 * L) + 4 * L
+                     for L, enc in links)
+    return {
+        "estimate_x_pass": 2 * Sc,
+        "forward_y_passes": 2 * Sc + N * 3 * Sc,
+        "forward_x_pass": N * 2 * Sc,
+        "detector": link_bytes + N * (2 * Sd + nin + St),
+        "adjoint_gather": N * St,
+        "scatter_x_pass": N * 2 * Sc,
+        "adjoint_y_x_passes": N * 5 * Sc + 4 * Sc,
+        "update": 4 * St,
+    }
+
+
 # DRAM bytes (read + write) over algorithmic bytes per spectral stage, from
 # the full-set ncu capture of the same kernels on c3 (4 x 1024^2 -> 2048^2,
 # FFT 3584^2): the kernels' traffic grows in proportion to the columns, rows
@@ -142,6 +171,14 @@ STAGE_LAUNCHES = {"estimate_x_pass": 1, "forward_y_passes": 1, "forward_x_pass":
 # ----------------------------------------------------------------------------- reference arm
 def reference_arm(args, rank, world):
     if rank != 0:
+        return 0
+    if args.workload == "pre":
+        cpu = preprocess_cpu_sample(_pre_exposures(), limit_s=40.0)
+        print(json.dumps({"impl": "reference", "metric": "ms/exposure (weight preprocessing)", "value": cpu["value"],
+                          "unit": "ms", "higher_is_better": False, "n_gpus": world, "steps": args.steps,
+                          "warmup": args.warmup, "config": {"workload": "pre", "shape": list(PRE_SHAPE)},
+                          "cpu_baseline": cpu, "e2e": {"value": cpu["value"], "unit": "ms",
+                                                       "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return 0
     from oracle import oracle as O
     from updc_b200 import synth
@@ -349,6 +386,108 @@ def batch_arm(args, rank, world, local_rank):
     return 0
 
 
+PRE_SHAPE, PRE_EXPOSURES = (2048, 2048), 8
+PRE_BYTES_PER_PIXEL = 4 + 4 + 8 + 8 + 8 + 4  # SCI, DQ, three variances read once; WHT written once
+
+
+def _pre_exposures():
+    from updc_b200 import synth
+    return [synth.level2_exposure(PRE_SHAPE, "sources", 100 + k) for k in range(PRE_EXPOSURES)]
+
+
+def _pre_planes(d):
+    import numpy as np
+    return (d["SCI"], d["DQ"], d["VAR_POISSON"].astype(np.float64), d["VAR_RNOISE"].astype(np.float64),
+            d["VAR_FLAT"].astype(np.float64))
+
+
+def preprocess_cpu_sample(exposures, limit_s=20.0):
+    """The oracle's restatement of the reference's NumPy preprocessing on as
+    many exposures as fit about `limit_s` seconds (at least one)."""
+    from oracle import preprocess as OP
+    t0 = time.time()
+    done = 0
+    for d in exposures:
+        OP.prepare_exposure(*_pre_planes(d), "rnoise-sky", 1, 0.0, "bench")
+        done += 1
+        if time.time() - t0 > limit_s:
+            break
+    ms = 1000.0 * (time.time() - t0) / done
+    return {"value": round(ms, 2), "unit": "ms", "cores": 1, "kind": "port",
+            "sample": f"{done} of {len(exposures)} exposures of {PRE_SHAPE[0]}x{PRE_SHAPE[1]} (NumPy, one thread)"}
+
+
+def preprocess_arm(args, rank, world, local_rank):
+    """Per-exposure weight preprocessing of the c1 exposures (8 x 2048^2
+    Level-2 planes): a step prepares every exposure; value = ms per exposure
+    with the planes resident on the device, e2e = the same through host
+    arrays (planes copied in, WHT copied out)."""
+    import numpy as np
+    import torch
+    from updc_b200 import preprocess as P
+    torch.cuda.set_device(local_rank)
+    exps = _pre_exposures()
+    host = [_pre_planes(d) for d in exps]
+    dev = []
+    for planes in host:
+        t = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in planes]
+        t[1] = t[1].view(torch.int32)
+        dev.append(t)
+    metrics = []
+    for _ in range(args.warmup):
+        for t in dev:
+            P.prepare_exposure(*t, "rnoise-sky", 1, 0.0, "bench")
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        start.record()
+        for _ in range(args.steps):
+            for t in dev:
+                _w, m, _s = P.prepare_exposure(*t, "rnoise-sky", 1, 0.0, "bench")
+                metrics.append(m)
+        stop.record()
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(stop) / (args.steps * len(dev))
+    if world > 1:
+        tt = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        ms = float(tt.item())
+    t0 = time.time()
+    e2e_steps = max(1, min(args.steps, 3))
+    for _ in range(e2e_steps):
+        for planes in host:
+            P.prepare_exposure(*planes, "rnoise-sky", 1, 0.0, "bench")
+    e2e_ms = 1000.0 * (time.time() - t0) / (e2e_steps * len(host))
+    npix = PRE_SHAPE[0] * PRE_SHAPE[1]
+    peak, peak_kind = measured_peaks()
+    achieved = PRE_BYTES_PER_PIXEL * npix / (ms * 1e-3) / 1e9
+    cpu = preprocess_cpu_sample(exps) if rank == 0 and world == 1 and not args.no_cpu_baseline else None
+    passes = statistics.mean(m["clip_passes"] for m in metrics)
+    result = {
+        "metric": "ms/exposure (weight preprocessing)", "value": round(ms, 4), "unit": "ms", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms * len(dev), 4),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": "pre", "exposures": len(dev), "shape": list(PRE_SHAPE), "weight_mode": "rnoise-sky",
+                   "clip_passes_mean": passes,
+                   "l2": "each exposure's planes (151 MB) exceed the 126 MB L2; 8 exposures cycle"},
+        "roofline": {"bound": "hbm", "kernel": "whole exposure (passes, sorts, host checks)",
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "peak_kind": peak_kind, "algorithmic_bytes": PRE_BYTES_PER_PIXEL * npix, "traffic": None},
+        "cpu_baseline": cpu,
+        "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": 32 * npix, "d2h_bytes_per_step": 4 * npix},
+        # k_pre_valid, k_pre_sky, k_pre_weight, k_pre_yeff, two order-statistic
+        # launches per clipping pass and the final one (sorts are CUB's)
+        "gpu_launches": int(round((5 + 2 * passes) * len(dev) * args.steps)),
+        "clocks": clocks.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(result))
+    return 0
+
+
 def sharded_arm(args, rank, world, local_rank):
     """N > 1: one field, its exposures split over the ranks (contiguous
     shares), every rank set up on the whole field; per iteration each rank
@@ -469,9 +608,12 @@ def b200_arm(args, rank, world, local_rank):
     stage_ms = {name: 1000.0 * statistics.mean(s.stage_seconds[i] for s in st) for i, name in enumerate(STAGES)}
     links = [(eng.link_count(k), eng.link_encoding(k)) for k in range(w.nexp)]
     sb = stage_bytes(w, fw, fh, links, [L for L, _ in links], 8 if args.form == "fp64" else 4)
+    mb = model_bytes(w, fw, fh, links, 8 if args.form == "fp64" else 4)
     dom = max(stage_ms, key=stage_ms.get)
     peak, peak_kind = measured_peaks()
-    achieved = sb[dom] / (stage_ms[dom] * 1e-3) / 1e9
+    achieved = mb[dom] / (stage_ms[dom] * 1e-3) / 1e9
+    achieved_pruned = sb[dom] / (stage_ms[dom] * 1e-3) / 1e9
+    iter_gbs = sum(mb.values()) / (ms * 1e-3) / 1e9
     # cuFFT (through torch) on the same padded grid, for comparison only: one
     # zero-padded 2-D R2C of the 4096^2 plane and one C2R + crop, as our
     # estimate/forward passes do them (not used by the solver)
@@ -512,10 +654,15 @@ def b200_arm(args, rank, world, local_rank):
         "wall_ms_per_step": round(1000.0 * wall / args.steps, 4),
         "setup_s": round(setup_s, 2),
         "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
-        "stage_gbs": {k: round(sb[k] / (stage_ms[k] * 1e-3) / 1e9, 1) for k in STAGES},
+        "stage_gbs": {k: round(mb[k] / (stage_ms[k] * 1e-3) / 1e9, 1) for k in STAGES},
+        "stage_gbs_pruned": {k: round(sb[k] / (stage_ms[k] * 1e-3) / 1e9, 1) for k in STAGES},
+        "iteration_model": {"bytes": sum(mb.values()), "achieved_gbs": round(iter_gbs, 1),
+                            "frac": round(iter_gbs / peak, 4)},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                     "algorithmic_bytes": sb[dom],
+                     "algorithmic_bytes": mb[dom],
+                     "pruned_bytes": sb[dom], "achieved_pruned": round(achieved_pruned, 1),
+                     "frac_pruned": round(achieved_pruned / peak, 4),
                      "traffic": round(sb[dom] * TRAFFIC_RATIO_C3[dom]) if dom in TRAFFIC_RATIO_C3 else None,
                      "traffic_source": "ncu dram__bytes_read+write of the c3 capture, scaled by units processed"},
         "cpu_baseline": cpu,
@@ -561,6 +708,8 @@ def main():
         return reference_arm(args, rank, world)
     if args.workload == "c2":
         return batch_arm(args, rank, world, local_rank)
+    if args.workload == "pre":
+        return preprocess_arm(args, rank, world, local_rank)
     if world > 1 and not args.replicas:
         return sharded_arm(args, rank, world, local_rank)
     return b200_arm(args, rank, world, local_rank)

@@ -232,6 +232,58 @@ int updc_psf_project_file(const char *input, int width, int height, const char *
                           int *out_width, int *out_height, double *input_sum, double *output_sum, uint64_t *overlaps,
                           char *message, size_t capacity);
 
+/* Per-exposure weight preprocessing on the GPU: the numeric part of the
+ * reference's Level-2 preparation, prepare_weighted_inputs.prepare_one
+ * (updc/_engine.py:349-397) with robust_background_mask (_engine.py:287-310)
+ * and build_weight (_engine.py:313-333), results identical to the reference's
+ * NumPy code.  Reading the FITS planes stays with the caller (the reference
+ * reads SCI, DQ, VAR_POISSON, VAR_RNOISE, VAR_FLAT with astropy).
+ *
+ * Status: 0; 1 with the reference's ValueError message in updc_last_error()
+ * ("Too few valid pixels for robust background estimation", "Cannot estimate
+ * a positive background RMS", "Cannot estimate sky VAR_POISSON", "No usable
+ * pixels remain in <source>", "Automatic pedestal failed to make y_eff
+ * positive in <source>"); 3 for an unknown weight mode, raised where the
+ * reference raises ValueError(mode), after the sky VAR_POISSON median; -2
+ * CUDA failure.  With device_pointers = 0 the planes are host arrays
+ * (copied in and out on `stream`); with 1 they are device pointers used on
+ * `stream` (a cudaStream_t; NULL = the legacy default stream). */
+enum { UPDC_WEIGHT_MASK = 0, UPDC_WEIGHT_RNOISE_SKY = 1, UPDC_WEIGHT_TOTALVAR = 2 };
+
+typedef struct updc_preprocess_metrics {
+    /* the metric record of _engine.py:387-398 */
+    double background;               /* sigma-clipped median of SCI */
+    double background_sigma;         /* 1.4826 x MAD of the clipped SCI */
+    double poisson_pedestal;         /* max(auto, requested) */
+    double auto_positivity_pedestal;
+    double requested_pedestal;
+    double min_valid_science;
+    double sky_var_poisson;          /* median VAR_POISSON over the sky mask */
+    double wht_valid_median;         /* median of the positive WHT values */
+    int64_t base_invalid;
+    int64_t nonpositive_valid_before_pedestal;
+    int64_t nonpositive_after_pedestal;
+    int64_t wht_zero;
+    /* diagnostics with no reference counterpart */
+    int32_t clip_passes;             /* clipping passes run (at most 6) */
+    int32_t std_fallbacks;           /* passes whose MAD was zero (standard deviation used) */
+} updc_preprocess_metrics;
+
+/* prepare_one's numeric steps for one exposure of npix pixels: WHT (float32,
+ * zero where unusable) to `wht`, the final sky mask (0/1) to `sky_mask` when
+ * not NULL, and the metrics.  `source` names the exposure in the messages. */
+int updc_preprocess_exposure(const float *science, const uint32_t *dq, const double *var_poisson,
+                             const double *var_rnoise, const double *var_flat, int64_t npix, int weight_mode,
+                             uint32_t bad_dq_mask, double pedestal_sigma, const char *source, float *wht,
+                             uint8_t *sky_mask, updc_preprocess_metrics *metrics, int device_pointers, void *stream);
+
+/* robust_background_mask (_engine.py:287-310): asymmetric sigma clipping of
+ * SCI over base_valid (0/1 bytes), at most max_iter passes; the final mask
+ * (0/1) to `mask`, the background and sigma of its last step. */
+int updc_robust_background(const float *science, const uint8_t *base_valid, int64_t npix, int max_iter,
+                           uint8_t *mask, double *background, double *sigma, int *passes, int device_pointers,
+                           void *stream);
+
 /* Geometry (overlap.c:72-116) and the known-answer self-test (updc_core.c:1545-1564). */
 float updc_polygon_area(const double *xy, int count);
 float updc_overlap_area(const double *quad8, int x, int y);

@@ -35,6 +35,15 @@ class IterStats(ctypes.Structure):
                 ("stage_seconds", ctypes.c_double * 8)]
 
 
+class PreprocessMetrics(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_double) for name in (
+        "background", "background_sigma", "poisson_pedestal", "auto_positivity_pedestal", "requested_pedestal",
+        "min_valid_science", "sky_var_poisson", "wht_valid_median")] + \
+        [(name, ctypes.c_int64) for name in ("base_invalid", "nonpositive_valid_before_pedestal",
+                                             "nonpositive_after_pedestal", "wht_zero")] + \
+        [("clip_passes", ctypes.c_int32), ("std_fallbacks", ctypes.c_int32)]
+
+
 class UpdcError(RuntimeError):
     """A failure reported by the engine; str() is the reference core's message."""
 
@@ -99,6 +108,10 @@ def load() -> ctypes.CDLL:
     L.updc_link_encoding.argtypes = [P, c.c_int]
     L.updc_decode_links.argtypes = [P, c.c_int, P]
     L.updc_build_linkmap.argtypes = [c.c_char_p, c.c_char_p] + [c.c_int] * 4 + [c.POINTER(c.c_uint64), c.POINTER(c.c_int)]
+    L.updc_preprocess_exposure.argtypes = [P, P, P, P, P, c.c_int64, c.c_int, c.c_uint32, c.c_double, c.c_char_p,
+                                           P, P, c.POINTER(PreprocessMetrics), c.c_int, P]
+    L.updc_robust_background.argtypes = [P, P, c.c_int64, c.c_int, P, c.POINTER(c.c_double),
+                                         c.POINTER(c.c_double), c.POINTER(c.c_int), c.c_int, P]
     L.updc_polygon_area.restype = c.c_float
     L.updc_polygon_area.argtypes = [P, c.c_int]
     L.updc_overlap_area.restype = c.c_float

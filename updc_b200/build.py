@@ -28,9 +28,9 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-r
               "-Xcompiler", "-Wall", "-I", str(ROOT / "include")]
 # geometry must not contract multiply-adds (bit-exact LinkMaps)
 PER_FILE = {"linkmap.cu": ["-fmad=false"], "projector.cu": ["-fmad=false"]}
-SOURCES = ["linkmap.cu", "engine.cu", "capi.cu", "noalloc.cu", "batch.cu", "projector.cu"]
+SOURCES = ["linkmap.cu", "engine.cu", "capi.cu", "noalloc.cu", "batch.cu", "projector.cu", "preprocess.cu"]
 HEADERS = ["common.cuh", "fft.cuh", "kernels.cuh", "pointwise.cuh", "engine.cuh", "geometry.cuh", "linkmap.cuh",
-           "tma.cuh", "nll.cuh"]
+           "tma.cuh", "nll.cuh", "preprocess.cuh"]
 
 
 def nvcc() -> str:

@@ -12,6 +12,7 @@
 #include "../../include/updc_b200.h"
 #include "engine.cuh"
 #include "linkmap.cuh"
+#include "preprocess.cuh"
 
 using namespace updc;
 
@@ -313,6 +314,28 @@ int updc_build_linkmap(const char *vertices, const char *links, int iw, int ih, 
         cudaStreamDestroy(s);
         if (nlinks) *nlinks = st.nlinks;
         if (encoding) *encoding = (int)st.encoding;
+    });
+}
+
+int updc_preprocess_exposure(const float *science, const uint32_t *dq, const double *var_poisson,
+                             const double *var_rnoise, const double *var_flat, int64_t npix, int weight_mode,
+                             uint32_t bad_dq_mask, double pedestal_sigma, const char *source, float *wht,
+                             uint8_t *sky_mask, updc_preprocess_metrics *metrics, int device_pointers, void *stream) {
+    return guarded([&] {
+        if (npix <= 0) throw Error(1, "invalid exposure size");
+        preprocess_exposure(science, dq, var_poisson, var_rnoise, var_flat, (size_t)npix, weight_mode, bad_dq_mask,
+                            pedestal_sigma, source ? source : "", wht, sky_mask, metrics, device_pointers != 0,
+                            (cudaStream_t)stream);
+    });
+}
+
+int updc_robust_background(const float *science, const uint8_t *base_valid, int64_t npix, int max_iter,
+                           uint8_t *mask, double *background, double *sigma, int *passes, int device_pointers,
+                           void *stream) {
+    return guarded([&] {
+        if (npix <= 0) throw Error(1, "invalid exposure size");
+        robust_background(science, base_valid, (size_t)npix, max_iter, mask, background, sigma, passes,
+                          device_pointers != 0, (cudaStream_t)stream);
     });
 }
 

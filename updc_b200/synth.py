@@ -394,3 +394,77 @@ def psf_projection_case(directory: os.PathLike, name: str, size: int, oversample
     np.stack((px, py), axis=-1).astype("<f8").tofile(f_vert)
     return f_psf, f_vert
 
+
+
+# ----------------------------------------------------------------------------- Level-2 exposures (weights)
+# Each case: (shape, weight_mode, bad_dq_mask, pedestal_sigma, pattern).  The
+# patterns exercise the branches of the per-exposure preprocessing: sources
+# above a noisy sky with bad DQ bits and non-finite pixels, each weight mode,
+# a requested pedestal, ties and an even number of clipped pixels, a MAD of
+# zero (standard-deviation fallback), and every failure the reference raises.
+PREPROCESS_CASES = {
+    "sky_sources": ((32, 40), "rnoise-sky", 1, 0.0, "sources"),
+    "totalvar_requested": ((48, 36), "totalvar", 5, 3.0, "sources"),
+    "mask_negative_sky": ((40, 40), "mask", 1, 0.0, "negative"),
+    "integer_ties": ((30, 44), "rnoise-sky", 1, 0.0, "ties"),
+    "mad_zero": ((36, 36), "rnoise-sky", 1, 0.0, "mad_zero"),
+    "too_few_valid": ((32, 32), "rnoise-sky", 1, 0.0, "too_few"),
+    "no_background_rms": ((32, 32), "rnoise-sky", 1, 0.0, "constant"),
+    "no_sky_var": ((32, 32), "rnoise-sky", 1, 0.0, "negative_var_p"),
+    "no_usable": ((32, 32), "rnoise-sky", 1, 0.0, "negative_var_r"),
+    "weight_underflow": ((32, 32), "rnoise-sky", 1, 0.0, "huge_var_r"),
+    "pedestal_fails": ((32, 32), "mask", 1, 0.0, "huge_negative"),
+    "unknown_mode": ((32, 32), "inverse-variance", 1, 0.0, "sources"),
+}
+
+
+def level2_exposure(shape, pattern: str, seed: int) -> dict:
+    """Synthetic Level-2 planes: SCI (f32), DQ (u32), VAR_POISSON, VAR_RNOISE,
+    VAR_FLAT (f32 as stored in the files; the preprocessing reads them as f64)."""
+    rng = np.random.default_rng(seed)
+    h, w = shape
+    n = h * w
+    sky = float(rng.uniform(0.2, 2.0))
+    rms = float(rng.uniform(0.5, 5.0))
+    sci = sky + rms * rng.standard_normal(n)
+    nsrc = max(1, n // 80)
+    idx = rng.choice(n, nsrc, replace=False)
+    sci[idx] += 10.0 ** rng.uniform(1.0, 4.0, nsrc)
+    dq = np.zeros(n, np.uint32)
+    dq[rng.choice(n, n // 50, replace=False)] = rng.choice([1, 2, 4, 1024], n // 50).astype(np.uint32)
+    var_p = np.abs(sci) * 1e-3 + 1e-4
+    var_r = np.full(n, rms * rms) * rng.uniform(0.9, 1.1, n)
+    var_f = np.full(n, 1e-4) * rng.uniform(0.5, 1.5, n)
+    if pattern == "negative":
+        sci -= 3.0 * sky + 4.0 * rms
+    elif pattern == "ties":
+        sci = np.round(sci)
+    elif pattern == "mad_zero":
+        sci[rng.random(n) < 0.6] = 2.0
+    elif pattern == "too_few":
+        dq[:] = 1
+        dq[rng.choice(n, 20, replace=False)] = 0
+    elif pattern == "constant":
+        sci[:] = 1.5
+    elif pattern == "negative_var_p":
+        var_p[:] = -1.0
+    elif pattern == "negative_var_r":
+        var_r[:] = -1.0e9
+    elif pattern == "huge_var_r":
+        var_r[:] = 1.0e300
+    elif pattern == "huge_negative":
+        sci[rng.integers(n)] = -1.0e20
+    sci = sci.astype(np.float32)
+    nonfinite = rng.choice(n, max(1, n // 200), replace=False)
+    if pattern not in ("constant", "too_few"):
+        sci[nonfinite[: len(nonfinite) // 2 + 1]] = np.nan
+        var_f[nonfinite[len(nonfinite) // 2:]] = np.inf
+    planes = {"SCI": sci, "DQ": dq, "VAR_POISSON": var_p.astype(np.float32), "VAR_RNOISE": var_r.astype(np.float64),
+              "VAR_FLAT": var_f.astype(np.float32)}
+    return {k: v.reshape(h, w) for k, v in planes.items()}
+
+
+def preprocess_case(name: str, index: int = 1) -> dict:
+    shape, _mode, _dqmask, _ped, pattern = PREPROCESS_CASES[name]
+    seed = 1000 + 17 * sorted(PREPROCESS_CASES).index(name) + index
+    return level2_exposure(shape, pattern, seed)
