@@ -420,14 +420,19 @@ def preprocess_cpu_sample(exposures, limit_s=20.0):
 def preprocess_arm(args, rank, world, local_rank):
     """Per-exposure weight preprocessing of the c1 exposures (8 x 2048^2
     Level-2 planes): a step prepares every exposure; value = ms per exposure
-    with the planes resident on the device, e2e = the same through host
-    arrays (planes copied in, WHT copied out)."""
+    with the planes resident on the device, e2e = the same through pinned
+    host arrays (planes copied in, WHT copied out)."""
     import numpy as np
     import torch
     from updc_b200 import preprocess as P
     torch.cuda.set_device(local_rank)
     exps = _pre_exposures()
-    host = [_pre_planes(d) for d in exps]
+
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=getattr(torch, a.dtype.name), pin_memory=True)
+        t.numpy()[...] = a
+        return t.numpy()
+    host = [tuple(pinned(np.ascontiguousarray(a)) for a in _pre_planes(d)) for d in exps]
     dev = []
     for planes in host:
         t = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in planes]
@@ -478,9 +483,10 @@ def preprocess_arm(args, rank, world, local_rank):
                      "peak_kind": peak_kind, "algorithmic_bytes": PRE_BYTES_PER_PIXEL * npix, "traffic": None},
         "cpu_baseline": cpu,
         "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": 32 * npix, "d2h_bytes_per_step": 4 * npix},
-        # k_pre_valid, k_pre_sky, k_pre_weight, k_pre_yeff, two order-statistic
-        # launches per clipping pass and the final one (sorts are CUB's)
-        "gpu_launches": int(round((5 + 2 * passes) * len(dev) * args.steps)),
+        # per exposure: k_pre_valid, k_pre_clip, k_pre_sky, k_pre_weight, two
+        # radix selects (1 + 2 x 8 and 1 + 2 x 4 launches); a standard-deviation
+        # fallback adds eight (the sort of SCI is CUB's)
+        "gpu_launches": int(sum(31 + 8 * m["std_fallbacks"] for m in metrics)),
         "clocks": clocks.summary(),
     }
     if rank == 0:

@@ -57,122 +57,159 @@ struct PreCounters {
     unsigned int pad;
 };
 
-// one atomic per block for a per-thread 0/1 count
-__device__ __forceinline__ void block_count(bool pred, unsigned long long *dst) {
-    __shared__ unsigned int s;
-    if (threadIdx.x == 0) s = 0;
-    __syncthreads();
-    const unsigned b = __ballot_sync(0xffffffffu, pred);
-    if ((threadIdx.x & 31) == 0 && b) atomicAdd(&s, (unsigned)__popc(b));
-    __syncthreads();
-    if (threadIdx.x == 0 && s) atomicAdd(dst, (unsigned long long)s);
+// A thread's count, summed over its warp, added with one atomic per warp.
+__device__ __forceinline__ void warp_add(unsigned count, unsigned long long *dst) {
+    const unsigned sum = __reduce_add_sync(0xffffffffu, count);
+    if ((threadIdx.x & 31) == 0 && sum) atomicAdd(dst, (unsigned long long)sum);
 }
 
 __device__ __forceinline__ float key_value(const uint32_t *sorted, unsigned long long i) {
     return ordered_to_float(sorted[i]);
 }
 
-// base_valid (_engine.py:356-360) and the sort keys of valid SCI
+// base_valid (_engine.py:356-360) and the sort keys of valid SCI.  Counting
+// kernels keep their counts in registers and add them once per warp; every
+// thread of a warp runs the same number of loop trips (n rounded up).
 __global__ void k_pre_valid(const float *__restrict__ sci, const uint32_t *__restrict__ dq,
                             const double *__restrict__ vp, const double *__restrict__ vr,
                             const double *__restrict__ vf, size_t n, uint32_t bad, int totalvar,
                             uint8_t *__restrict__ valid, uint32_t *__restrict__ keys, PreCounters *cnt) {
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
-    const size_t n_round = ceil_div(n, blockDim.x) * blockDim.x;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n_round; i += stride) {
-        bool ok = false;
-        if (i < n) {
-            const float s = sci[i];
-            ok = isfinite(s) && (dq[i] & bad) == 0 && isfinite(vp[i]) && isfinite(vr[i]) &&
-                 (!totalvar || isfinite(vf[i]));
-            valid[i] = ok;
-            keys[i] = ok ? float_to_ordered(s) : 0xFFFFFFFFu;
-        }
-        block_count(ok, &cnt->valid);
+    unsigned c = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float s = sci[i];
+        const bool ok = isfinite(s) && (dq[i] & bad) == 0 && isfinite(vp[i]) && isfinite(vr[i]) &&
+                        (!totalvar || isfinite(vf[i]));
+        valid[i] = ok;
+        keys[i] = ok ? float_to_ordered(s) : 0xFFFFFFFFu;
+        c += ok;
     }
+    warp_add(c, &cnt->valid);
 }
 
 // the same keys from a caller-given base_valid mask
 __global__ void k_pre_keys(const float *__restrict__ sci, const uint8_t *__restrict__ valid, size_t n,
                            uint32_t *__restrict__ keys, PreCounters *cnt) {
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
-    const size_t n_round = ceil_div(n, blockDim.x) * blockDim.x;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n_round; i += stride) {
-        bool ok = false;
-        if (i < n) {
-            ok = valid[i] != 0;
-            keys[i] = ok ? float_to_ordered(sci[i]) : 0xFFFFFFFFu;
-        }
-        block_count(ok, &cnt->valid);
+    unsigned c = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const bool ok = valid[i] != 0;
+        keys[i] = ok ? float_to_ordered(sci[i]) : 0xFFFFFFFFu;
+        c += ok;
     }
+    warp_add(c, &cnt->valid);
 }
 
-// first index in [lo, hi) whose value is > x (strict = true) or >= x
-__device__ unsigned long long sorted_bound(const uint32_t *s, unsigned long long lo, unsigned long long hi, float x,
-                                           bool strict) {
-    while (lo < hi) {
-        const unsigned long long mid = lo + (hi - lo) / 2;
-        const float v = key_value(s, mid);
-        if (strict ? (v > x) : (v >= x))
-            hi = mid;
-        else
-            lo = mid + 1;
+// Smallest i in [lo, hi) with pred(i) true (pred goes false -> true once),
+// or hi.  One warp: each round the 32 lanes test the last element of 32
+// equal chunks and the search continues in the first chunk that ends true,
+// so a range of 2^22 takes five rounds of loads instead of 22.
+template <class Pred>
+__device__ unsigned long long warp_first_true(unsigned long long lo, unsigned long long hi, Pred pred) {
+    const unsigned lane = threadIdx.x & 31;
+    while (hi - lo > 32) {
+        const unsigned long long len = hi - lo, step = (len + 31) / 32;
+        const unsigned long long end = min((unsigned long long)(lane + 1) * step, len);
+        const unsigned m = __ballot_sync(0xffffffffu, pred(lo + end - 1));
+        if (!m) return hi;
+        const unsigned f = __ffs(m) - 1;
+        hi = lo + min((unsigned long long)(f + 1) * step, len);
+        lo += (unsigned long long)f * step;
     }
-    return lo;
+    const unsigned long long i = lo + lane;
+    const unsigned m = __ballot_sync(0xffffffffu, i < hi && pred(i));
+    return m ? lo + (__ffs(m) - 1) : hi;
 }
-
-struct CenterOut {
-    float med, mad;
-};
 
 // k-th smallest (0-based) of |fl32(v - med)| over sorted[a, b), split at p
 // (values <= med before p): run A walks down from p-1, run B up from p, both
-// with non-decreasing deviations; merge-path search for the split.
-__device__ float kth_deviation(const uint32_t *s, unsigned long long a, unsigned long long b, unsigned long long p,
-                               float med, unsigned long long k) {
+// with non-decreasing deviations; merge-path search for how many of the k+1
+// smallest come from A.
+__device__ float warp_kth_deviation(const uint32_t *s, unsigned long long a, unsigned long long b,
+                                    unsigned long long p, float med, unsigned long long k) {
     const unsigned long long la = p - a, lb = b - p;
     auto A = [&](unsigned long long j) { return fabsf(__fsub_rn(key_value(s, p - 1 - j), med)); };
     auto B = [&](unsigned long long j) { return fabsf(__fsub_rn(key_value(s, p + j), med)); };
-    unsigned long long lo = (k + 1 > lb) ? k + 1 - lb : 0, hi = (k + 1 < la) ? k + 1 : la;
-    while (lo < hi) {
-        const unsigned long long i = lo + (hi - lo) / 2;
-        if (A(i) < B(k - i))
-            lo = i + 1;
-        else
-            hi = i;
-    }
-    const unsigned long long i = lo, j = k + 1 - lo;
+    const unsigned long long lo = (k + 1 > lb) ? k + 1 - lb : 0, hi = (k + 1 < la) ? k + 1 : la;
+    const unsigned long long i = warp_first_true(lo, hi, [&](unsigned long long t) { return !(A(t) < B(k - t)); });
+    const unsigned long long j = k + 1 - i;
     float r = -INFINITY;
     if (i > 0) r = A(i - 1);
     if (j > 0) r = fmaxf(r, B(j - 1));
     return r;
 }
 
-// median and MAD of sorted[a, b) (numpy.median semantics in float32)
-__global__ void k_pre_center(const uint32_t *__restrict__ s, unsigned long long a, unsigned long long b,
-                             CenterOut *out) {
-    if (blockIdx.x || threadIdx.x) return;
+// median and MAD of sorted[a, b), b > a (numpy.median semantics in float32)
+__device__ void warp_center(const uint32_t *s, unsigned long long a, unsigned long long b, float *med_out,
+                            float *mad_out) {
     const unsigned long long m = b - a, k1 = (m - 1) / 2, k2 = m / 2;
     const float v1 = key_value(s, a + k1), v2 = key_value(s, a + k2);
     const float med = (m & 1) ? v1 : __fdiv_rn(__fadd_rn(v1, v2), 2.0f);
-    const unsigned long long p = sorted_bound(s, a, b, med, true);
-    const float d1 = kth_deviation(s, a, b, p, med, k1);
-    const float d2 = (m & 1) ? d1 : kth_deviation(s, a, b, p, med, k2);
-    out->med = med;
-    out->mad = (m & 1) ? d1 : __fdiv_rn(__fadd_rn(d1, d2), 2.0f);
+    const unsigned long long p = warp_first_true(a, b, [&](unsigned long long i) { return key_value(s, i) > med; });
+    const float d1 = warp_kth_deviation(s, a, b, p, med, k1);
+    const float d2 = (m & 1) ? d1 : warp_kth_deviation(s, a, b, p, med, k2);
+    *med_out = med;
+    *mad_out = (m & 1) ? d1 : __fdiv_rn(__fadd_rn(d1, d2), 2.0f);
 }
 
-struct RangeOut {
-    unsigned long long a, b;
+enum ClipStatus : int { CLIP_RUN = 0, CLIP_DONE = 1, CLIP_TOO_FEW = 2, CLIP_NEED_STD = 3, CLIP_NO_RMS = 4 };
+
+struct ClipState {
+    unsigned long long a, b;  // current mask = sorted range [a, b) of the valid values
+    int it, passes, fallbacks, status, windowed;
+    float lo, hi;             // window of the current mask (windowed = 0: the mask is base_valid)
+    double background, sigma;
 };
 
-// sorted range of the window lo < v < hi over the valid values [0, nv)
-__global__ void k_pre_window(const uint32_t *__restrict__ s, unsigned long long nv, float lo, float hi,
-                             RangeOut *out) {
-    if (blockIdx.x || threadIdx.x) return;
-    const unsigned long long a = sorted_bound(s, 0, nv, lo, true), b = sorted_bound(s, 0, nv, hi, false);
-    out->a = b > a ? a : 0;
-    out->b = b > a ? b : 0;
+// The clipping loop of _engine.py:293-310 on the sorted valid SCI, one warp.
+// It stops with CLIP_NEED_STD when a pass's MAD is zero; the host then
+// computes numpy.std of the current mask and relaunches with it.
+__global__ void k_pre_clip(const uint32_t *__restrict__ s, unsigned long long nv, unsigned long long need,
+                           int max_iter, ClipState *state, int has_std, float std_value) {
+    ClipState c = *state;
+    c.status = CLIP_RUN;
+    for (; c.it < max_iter; ++c.it) {
+        if (c.b - c.a < need) {
+            c.status = CLIP_TOO_FEW;
+            break;
+        }
+        float med, mad;
+        warp_center(s, c.a, c.b, &med, &mad);
+        double sig = __dmul_rn(MAD_TO_SIGMA, (double)mad);
+        if (!(isfinite(sig) && sig > 0.0)) {
+            if (!has_std) {
+                c.status = CLIP_NEED_STD;
+                break;
+            }
+            has_std = 0;
+            sig = (double)std_value;
+            ++c.fallbacks;
+        }
+        if (!(isfinite(sig) && sig > 0.0)) {
+            c.status = CLIP_NO_RMS;
+            break;
+        }
+        ++c.passes;
+        // float64 bounds rounded to float32 for the float32 comparison
+        c.lo = __double2float_rn(__dsub_rn((double)med, __dmul_rn(CLIP_LOW, sig)));
+        c.hi = __double2float_rn(__dadd_rn((double)med, __dmul_rn(CLIP_HIGH, sig)));
+        c.windowed = 1;
+        const float lo = c.lo, hi = c.hi;
+        unsigned long long a = warp_first_true(0, nv, [&](unsigned long long i) { return key_value(s, i) > lo; });
+        unsigned long long b = warp_first_true(0, nv, [&](unsigned long long i) { return key_value(s, i) >= hi; });
+        if (b <= a) a = b = 0;  // empty masks compare equal
+        const bool same = a == c.a && b == c.b;
+        c.a = a;
+        c.b = b;
+        if (same) break;
+    }
+    if (c.status == CLIP_RUN) {
+        float med = NAN, mad = NAN;  // numpy.median of nothing
+        if (c.b > c.a) warp_center(s, c.a, c.b, &med, &mad);
+        c.background = med;
+        // the final MAD stays float32, so 1.4826 is rounded to float32 too
+        c.sigma = (double)__fmul_rn((float)MAD_TO_SIGMA, mad);
+        c.status = CLIP_DONE;
+    }
+    if (threadIdx.x == 0) *state = c;
 }
 
 // flags of the pixels in the current clipping mask (pixel order)
@@ -290,20 +327,17 @@ __global__ void k_pre_sqdev(const float *__restrict__ v, unsigned long long n, f
 __global__ void k_pre_sky(const float *__restrict__ sci, const uint8_t *__restrict__ valid,
                           const double *__restrict__ vp, size_t n, float lo, float hi, uint8_t *__restrict__ sky,
                           unsigned long long *__restrict__ keys, PreCounters *cnt) {
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
-    const size_t n_round = ceil_div(n, blockDim.x) * blockDim.x;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n_round; i += stride) {
-        bool take = false;
-        if (i < n) {
-            const float s = sci[i];
-            const bool in = valid[i] && s > lo && s < hi;
-            if (sky) sky[i] = in;
-            const double v = vp[i];
-            take = in && isfinite(v) && v >= 0.0;
-            keys[i] = take ? double_to_ordered(v) : ~0ull;
-        }
-        block_count(take, &cnt->sky);
+    unsigned c = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float s = sci[i];
+        const bool in = valid[i] && s > lo && s < hi;
+        if (sky) sky[i] = in;
+        const double v = vp[i];
+        const bool take = in && isfinite(v) && v >= 0.0;
+        keys[i] = take ? double_to_ordered(v) : ~0ull;
+        c += take;
     }
+    warp_add(c, &cnt->sky);
 }
 
 // weights of the mode (_engine.py:317-332), the usable mask (in place of
@@ -312,49 +346,144 @@ __global__ void k_pre_weight(const float *__restrict__ sci, uint8_t *__restrict_
                              const double *__restrict__ vp, const double *__restrict__ vr,
                              const double *__restrict__ vf, size_t n, int mode, double sky_var_p,
                              float *__restrict__ wht, uint32_t *__restrict__ wkeys, PreCounters *cnt) {
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
-    const size_t n_round = ceil_div(n, blockDim.x) * blockDim.x;
-    __shared__ unsigned int smin;
-    if (threadIdx.x == 0) smin = 0xFFFFFFFFu;
-    __syncthreads();
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n_round; i += stride) {
-        bool usable = false, nonpos = false, zero = false, pos = false;
-        if (i < n) {
-            double w;
-            if (mode == WM_MASK)
-                w = 1.0;
-            else if (mode == WM_RNOISE_SKY)
-                w = __ddiv_rn(1.0, __dadd_rn(vr[i], sky_var_p));
-            else
-                w = __ddiv_rn(1.0, __dadd_rn(__dadd_rn(vp[i], vr[i]), vf[i]));
-            const float s = sci[i];
-            usable = valid_usable[i] && isfinite(w) && w > 0.0;
-            valid_usable[i] = usable;
-            nonpos = usable && s <= 0.0f;
-            const float o = usable ? __double2float_rn(w) : 0.0f;
-            wht[i] = o;
-            zero = o == 0.0f;
-            pos = o > 0.0f;
-            wkeys[i] = pos ? __float_as_uint(o) : 0xFFFFFFFFu;
-            if (usable) atomicMin(&smin, float_to_ordered(s));
-        }
-        block_count(usable, &cnt->usable);
-        block_count(nonpos, &cnt->nonpos_before);
-        block_count(zero, &cnt->wht_zero);
-        block_count(pos, &cnt->wht_pos);
+    unsigned n_usable = 0, n_nonpos = 0, n_zero = 0, n_pos = 0, kmin = 0xFFFFFFFFu;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        double w;
+        if (mode == WM_MASK)
+            w = 1.0;
+        else if (mode == WM_RNOISE_SKY)
+            w = __ddiv_rn(1.0, __dadd_rn(vr[i], sky_var_p));
+        else
+            w = __ddiv_rn(1.0, __dadd_rn(__dadd_rn(vp[i], vr[i]), vf[i]));
+        const float s = sci[i];
+        const bool usable = valid_usable[i] && isfinite(w) && w > 0.0;
+        valid_usable[i] = usable;
+        const float o = usable ? __double2float_rn(w) : 0.0f;
+        wht[i] = o;
+        wkeys[i] = o > 0.0f ? __float_as_uint(o) : 0xFFFFFFFFu;
+        n_usable += usable;
+        n_nonpos += usable && s <= 0.0f;
+        n_zero += o == 0.0f;
+        n_pos += o > 0.0f;
+        if (usable) kmin = min(kmin, float_to_ordered(s));
     }
-    __syncthreads();
-    if (threadIdx.x == 0 && smin != 0xFFFFFFFFu) atomicMin(&cnt->min_usable_key, smin);
+    warp_add(n_usable, &cnt->usable);
+    warp_add(n_nonpos, &cnt->nonpos_before);
+    warp_add(n_zero, &cnt->wht_zero);
+    warp_add(n_pos, &cnt->wht_pos);
+    kmin = __reduce_min_sync(0xffffffffu, kmin);
+    if ((threadIdx.x & 31) == 0 && kmin != 0xFFFFFFFFu) atomicMin(&cnt->min_usable_key, kmin);
 }
 
-__global__ void k_pre_yeff(const float *__restrict__ sci, const uint8_t *__restrict__ usable, size_t n,
-                           double pedestal, PreCounters *cnt) {
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
-    const size_t n_round = ceil_div(n, blockDim.x) * blockDim.x;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n_round; i += stride) {
-        bool bad = false;
-        if (i < n) bad = usable[i] && __dadd_rn((double)sci[i], pedestal) <= 0.0;
-        block_count(bad, &cnt->nonpos_after);
+// ---- exact selection of the two middle order statistics of a key array
+// (numpy.median's pair) without sorting: MSB-first radix select over 11-bit
+// digits for both ranks at once.  Each pass histograms the keys that match
+// the digits fixed so far; the last block of the pass to finish (a ticket
+// counter, no waiting) fixes the next digit of each rank and clears the
+// histograms for the next pass.  Keys equal to the all-ones sentinel mark
+// non-participants and sort last, so they are never selected.
+constexpr int SEL_BITS = 11, SEL_BINS = 1 << SEL_BITS;
+
+template <typename K> struct SelectState {
+    K prefix[2];
+    unsigned long long rank[2];
+    unsigned split;  // the two ranks' prefixes differ in the digits fixed so far
+    unsigned ticket;
+};
+
+template <typename K>
+__global__ void k_sel_init(SelectState<K> *st, const unsigned long long *count, unsigned *hist) {
+    const unsigned long long m = *count;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->prefix[0] = st->prefix[1] = 0;
+        st->rank[0] = m ? (m - 1) / 2 : 0;
+        st->rank[1] = m / 2;
+        st->split = 0;
+        st->ticket = 0;
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 2 * SEL_BINS; i += gridDim.x * blockDim.x) hist[i] = 0;
+}
+
+// fix digit [shift, shift + width) of rank r from histogram h (SEL_PICK_NT threads)
+constexpr int SEL_PICK_NT = 256, SEL_PER_THREAD = SEL_BINS / SEL_PICK_NT;
+
+template <typename K>
+__device__ void sel_fix_digit(SelectState<K> *st, int r, const unsigned *h, int shift, int width) {
+    using Scan = cub::BlockScan<unsigned long long, SEL_PICK_NT>;
+    __shared__ typename Scan::TempStorage tmp;
+    __shared__ int digit;
+    __shared__ unsigned long long below;
+    const int t = threadIdx.x, nb = 1 << width;
+    unsigned c[SEL_PER_THREAD];
+    unsigned long long mine = 0;
+#pragma unroll
+    for (int j = 0; j < SEL_PER_THREAD; ++j) {
+        const int b = t * SEL_PER_THREAD + j;
+        c[j] = b < nb ? __ldcg(h + b) : 0u;
+        mine += c[j];
+    }
+    unsigned long long excl;
+    Scan(tmp).ExclusiveSum(mine, excl);
+    const unsigned long long rank = st->rank[r];
+    if (rank >= excl && rank < excl + mine) {
+        unsigned long long run = excl;
+#pragma unroll
+        for (int j = 0; j < SEL_PER_THREAD; ++j) {
+            if (rank >= run && rank < run + c[j]) {
+                digit = t * SEL_PER_THREAD + j;
+                below = run;
+            }
+            run += c[j];
+        }
+    }
+    __syncthreads();
+    if (t == 0) {
+        st->rank[r] = rank - below;
+        st->prefix[r] |= (K)digit << shift;
+    }
+    __syncthreads();
+}
+
+template <typename K>
+__global__ void __launch_bounds__(SEL_PICK_NT) k_sel_pass(const K *__restrict__ keys, size_t n, SelectState<K> *st,
+                                                          int shift, int width, unsigned *hist) {
+    __shared__ unsigned h[2 * SEL_BINS];
+    __shared__ bool last;
+    for (int i = threadIdx.x; i < 2 * SEL_BINS; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    const int bits = 8 * (int)sizeof(K);
+    const K above = shift + width >= bits ? K(0) : (~K(0) << (shift + width));
+    const K p0 = st->prefix[0] & above, p1 = st->prefix[1] & above;
+    const bool split = st->split != 0;
+    const unsigned dmask = (1u << width) - 1u;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const K k = keys[i];
+        const unsigned d = (unsigned)(k >> shift) & dmask;
+        const K hk = k & above;
+        if (hk == p0) {
+            const unsigned peers = __match_any_sync(__activemask(), d);
+            if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&h[d], (unsigned)__popc(peers));
+        }
+        if (split && hk == p1) {
+            const unsigned peers = __match_any_sync(__activemask(), d);
+            if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&h[SEL_BINS + d], (unsigned)__popc(peers));
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 2 * SEL_BINS; i += blockDim.x)
+        if (h[i]) atomicAdd(&hist[i], h[i]);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&st->ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    sel_fix_digit(st, 0, hist, shift, width);
+    sel_fix_digit(st, 1, hist + (split ? SEL_BINS : 0), shift, width);
+    for (int i = threadIdx.x; i < 2 * SEL_BINS; i += blockDim.x) hist[i] = 0;
+    if (threadIdx.x == 0) {
+        st->split = st->prefix[0] != st->prefix[1];
+        st->ticket = 0;
     }
 }
 
@@ -458,10 +587,25 @@ template <typename K> void sort_keys(const K *keys, K *sorted, size_t n, Scratch
     UPDC_CUDA(cub::DeviceRadixSort::SortKeys(tmp, tb, keys, sorted, (int)n, 0, 8 * (int)sizeof(K), st));
 }
 
-// the two middle order statistics of the first m sorted keys
-template <typename K> void middle_pair(const K *sorted, unsigned long long m, K *lo, K *hi, cudaStream_t st) {
-    to_host(lo, sorted + (m - 1) / 2, 1, st);
-    to_host(hi, sorted + m / 2, 1, st);
+// the two middle order statistics (ranks (m-1)/2 and m/2) of the m keys that
+// are not the sentinel; `count` is m on the device
+template <typename K>
+void middle_pair(const K *keys, size_t n, const unsigned long long *count, K *lo, K *hi, Scratch &S,
+                 cudaStream_t st) {
+    SelectState<K> *dst = S.get<SelectState<K>>(1);
+    unsigned *hist = S.get<unsigned>(2 * SEL_BINS);
+    k_sel_init<K><<<8, 256, 0, st>>>(dst, count, hist);
+    const unsigned g = pre_grid(n);
+    for (int top = 8 * (int)sizeof(K); top > 0;) {
+        const int shift = std::max(0, top - SEL_BITS), width = top - shift;
+        k_sel_pass<K><<<g, SEL_PICK_NT, 0, st>>>(keys, n, dst, shift, width, hist);
+        top = shift;
+    }
+    UPDC_CUDA(cudaGetLastError());
+    SelectState<K> h;
+    to_host(&h, dst, 1, st);
+    *lo = h.prefix[0];
+    *hi = h.prefix[1];
 }
 
 // robust_background_mask (_engine.py:287-310) over device SCI and base_valid;
@@ -469,48 +613,36 @@ template <typename K> void middle_pair(const K *sorted, unsigned long long m, K 
 ClipResult robust_clip(const float *sci, const uint8_t *valid, const uint32_t *keys, size_t n, int max_iter,
                        PreCounters *dcnt, Scratch &S, cudaStream_t st) {
     uint32_t *sorted = S.get<uint32_t>(n);
-    CenterOut *dc = S.get<CenterOut>(1);
-    RangeOut *dr = S.get<RangeOut>(1);
+    ClipState *dstate = S.get<ClipState>(1);
     sort_keys(keys, sorted, n, S, st);
     PreCounters hc;
     to_host(&hc, dcnt, 1, st);
     const unsigned long long nv = hc.valid;
     const unsigned long long need = std::max<unsigned long long>(32, std::min<unsigned long long>(1000, n / 100));
-    ClipResult r;
-    unsigned long long a = 0, b = nv;
-    auto center = [&](unsigned long long a_, unsigned long long b_) {
-        CenterOut c{NAN, NAN};  // numpy.median of nothing
-        if (b_ > a_) {
-            k_pre_center<<<1, 1, 0, st>>>(sorted, a_, b_, dc);
-            to_host(&c, dc, 1, st);
-        }
-        return c;
-    };
-    for (int it = 0; it < max_iter; ++it) {
-        if (b - a < need) throw Error(1, "Too few valid pixels for robust background estimation");
-        const CenterOut c = center(a, b);
-        const double med = c.med;
-        double sig = MAD_TO_SIGMA * (double)c.mad;
-        if (!(std::isfinite(sig) && sig > 0)) {
-            ++r.fallbacks;
-            sig = (double)masked_std(sci, valid, n, r.windowed, r.lo, r.hi, S, st);
-        }
-        if (!(std::isfinite(sig) && sig > 0)) throw Error(1, "Cannot estimate a positive background RMS");
-        ++r.passes;
-        r.lo = (float)(med - CLIP_LOW * sig);
-        r.hi = (float)(med + CLIP_HIGH * sig);
-        r.windowed = true;
-        k_pre_window<<<1, 1, 0, st>>>(sorted, nv, r.lo, r.hi, dr);
-        RangeOut w;
-        to_host(&w, dr, 1, st);
-        const bool same = w.a == a && w.b == b;  // empty ranges are normalised to [0, 0)
-        a = w.a;
-        b = w.b;
-        if (same) break;
+    ClipState c = {};
+    c.a = 0;
+    c.b = nv;
+    UPDC_CUDA(cudaMemcpyAsync(dstate, &c, sizeof(c), cudaMemcpyHostToDevice, st));
+    int has_std = 0;
+    float std_value = 0.0f;
+    for (;;) {
+        k_pre_clip<<<1, 32, 0, st>>>(sorted, nv, need, max_iter, dstate, has_std, std_value);
+        UPDC_CUDA(cudaGetLastError());
+        to_host(&c, dstate, 1, st);
+        if (c.status == CLIP_TOO_FEW) throw Error(1, "Too few valid pixels for robust background estimation");
+        if (c.status == CLIP_NO_RMS) throw Error(1, "Cannot estimate a positive background RMS");
+        if (c.status != CLIP_NEED_STD) break;
+        std_value = masked_std(sci, valid, n, c.windowed != 0, c.lo, c.hi, S, st);
+        has_std = 1;
     }
-    const CenterOut c = center(a, b);
-    r.background = c.med;
-    r.sigma = (double)((float)MAD_TO_SIGMA * c.mad);
+    ClipResult r;
+    r.lo = c.lo;
+    r.hi = c.hi;
+    r.windowed = c.windowed != 0;
+    r.background = c.background;
+    r.sigma = c.sigma;
+    r.passes = c.passes;
+    r.fallbacks = c.fallbacks;
     return r;
 }
 
@@ -548,16 +680,15 @@ void preprocess_device(const DeviceInputs &in, size_t n, int mode, uint32_t bad,
     const ClipResult clip = robust_clip(in.sci, valid, keys, n, 6, dcnt, S, st);
 
     // build_weight: sky VAR_POISSON median (_engine.py:315-317)
-    unsigned long long *k64 = S.get<unsigned long long>(n), *s64 = S.get<unsigned long long>(n);
+    unsigned long long *k64 = S.get<unsigned long long>(n);
     k_pre_sky<<<g, PRE_NT, 0, st>>>(in.sci, valid, in.vp, n, clip.lo, clip.hi, sky, k64, dcnt);
     UPDC_CUDA(cudaGetLastError());
     PreCounters hc;
     to_host(&hc, dcnt, 1, st);
     double sky_var_p = NAN;
     if (hc.sky) {
-        sort_keys(k64, s64, n, S, st);
         unsigned long long lo = 0, hi = 0;
-        middle_pair(s64, hc.sky, &lo, &hi, st);
+        middle_pair(k64, n, &dcnt->sky, &lo, &hi, S, st);
         const double v1 = ordered_to_double(lo), v2 = ordered_to_double(hi);
         sky_var_p = (hc.sky & 1) ? v1 : (v1 + v2) / 2.0;
     }
@@ -575,17 +706,15 @@ void preprocess_device(const DeviceInputs &in, size_t n, int mode, uint32_t bad,
     const double auto_ped = py_max(0.0, floor_ - min_valid);
     const double requested = py_max(0.0, pedestal_sigma * clip.sigma - clip.background);
     const double pedestal = py_max(auto_ped, requested);
-    k_pre_yeff<<<g, PRE_NT, 0, st>>>(in.sci, valid, n, pedestal, dcnt);
-    UPDC_CUDA(cudaGetLastError());
-    to_host(&hc, dcnt, 1, st);
-    if (hc.nonpos_after) throw Error(1, "Automatic pedestal failed to make y_eff positive in " + source);
+    // y_eff = SCI + pedestal (float64) is monotonic in SCI, so a usable pixel
+    // with y_eff <= 0 exists exactly when the smallest usable SCI gives one;
+    // the reference raises before reporting how many
+    if (min_valid + pedestal <= 0.0) throw Error(1, "Automatic pedestal failed to make y_eff positive in " + source);
     if (hc.wht_pos == 0) throw Error(1, "No usable pixels remain in " + source);
 
     // median of the positive WHT values (_engine.py:393)
-    uint32_t *ws = S.get<uint32_t>(n);
-    sort_keys(keys, ws, n, S, st);
     uint32_t lo = 0, hi = 0;
-    middle_pair(ws, hc.wht_pos, &lo, &hi, st);
+    middle_pair(keys, n, &dcnt->wht_pos, &lo, &hi, S, st);
     float w1, w2;
     memcpy(&w1, &lo, 4);
     memcpy(&w2, &hi, 4);
@@ -601,7 +730,7 @@ void preprocess_device(const DeviceInputs &in, size_t n, int mode, uint32_t bad,
     M->wht_valid_median = (double)wmed;
     M->base_invalid = (int64_t)(n - hc.valid);
     M->nonpositive_valid_before_pedestal = (int64_t)hc.nonpos_before;
-    M->nonpositive_after_pedestal = (int64_t)hc.nonpos_after;
+    M->nonpositive_after_pedestal = 0;
     M->wht_zero = (int64_t)hc.wht_zero;
     M->clip_passes = clip.passes;
     M->std_fallbacks = clip.fallbacks;
