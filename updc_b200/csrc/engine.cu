@@ -138,8 +138,10 @@ template <typename T> std::vector<cx<T>> fft_make_table(int n, const std::vector
         plan.twoff[s] = (int)tab.size();
         plan.ns_div[s] = FastDiv((uint32_t)ns);
         plan.nb_div[s] = FastDiv((uint32_t)(n / R));
-        for (int k = 0; k < ns; ++k)
-            for (int r = 1; r < R; ++r) {
+        // r-major: the twiddles of input r for consecutive k are adjacent, so
+        // the lanes of a warp (consecutive k) load them coalesced
+        for (int r = 1; r < R; ++r)
+            for (int k = 0; k < ns; ++k) {
                 const double a = -two_pi * (double)r * (double)k / ((double)ns * (double)R);
                 tab.push_back(cx<T>{(T)std::cos(a), (T)std::sin(a)});
             }

@@ -354,10 +354,10 @@ __device__ __forceinline__ void fft_stage(cx<T> *buf, int n, int batch, int Ns, 
 #pragma unroll
             for (int r = 0; r < R; ++r) v[kk][r] = buf[fpad(base + r * nb, sh)];
             if (k) {
-                const cx<T> *t = tw + k * (R - 1);
+                const cx<T> *t = tw + k;
 #pragma unroll
                 for (int r = 1; r < R; ++r) {
-                    cx<T> w = t[r - 1];
+                    cx<T> w = t[(r - 1) * Ns];
                     if (INV) w.y = -w.y;
                     v[kk][r] = fmulc(v[kk][r], w);
                 }
