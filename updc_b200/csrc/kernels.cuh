@@ -258,6 +258,15 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
 // All transforms go through one forward-FFT call site; the inverse is
 // conj(FFT(conj(.))), which keeps a single inlined copy of the FFT (two
 // copies make ptxas spill).
+// Asks L2 to fetch [p, p + bytes) of this GPU's memory ahead of its use
+// (bulk prefetch, no destination; the range is rounded inwards to 16 bytes).
+__device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes) {
+    uintptr_t a = (uintptr_t)p, e = a + bytes;
+    a = (a + 15) & ~(uintptr_t)15;
+    e &= ~(uintptr_t)15;
+    if (e > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((uint32_t)(e - a)) : "memory");
+}
+
 template <typename T, int NT, int CAP>
 __device__ __forceinline__ void col_forward_column(const FftPlan &plan, const cx<T> *__restrict__ rx, int ldr,
                                                    int rows_in, const cx<T> *__restrict__ khat, size_t khat_stride,
@@ -269,6 +278,8 @@ __device__ __forceinline__ void col_forward_column(const FftPlan &plan, const cx
     const cx<T> *src = rx + (size_t)u * ldr;
 #pragma unroll 1
     for (int it = 0; it <= nexp; ++it) {
+        // the OTF column of the next exposure is fetched into L2 during this FFT
+        if (threadIdx.x == 0 && it < nexp) prefetch_l2(khat + it * khat_stride + (size_t)u * n, (size_t)n * sizeof(cx<T>));
         if (it == 0) {
             for (int v = threadIdx.x; v < n; v += NT) buf[fpad(v, sh)] = v < rows_in ? src[v] : cx<T>{0, 0};
         } else {
