@@ -236,6 +236,7 @@ namespace {
 constexpr int NT = SPEC_NT;
 template <typename T> using NtAdj = SpecNtAdj<T>;
 template <typename T> using ColNt = SpecColNt<T>;
+template <typename T> using RowNt = SpecRowNt<T>;
 template <typename T> using Caps = SpecCaps<T>;
 constexpr size_t SMEM_LIMIT = SPEC_SMEM_LIMIT;
 
@@ -690,9 +691,9 @@ template <typename T> class EngineImpl final : public Engine {
         const PsfWindowStore<T> epi{d_psf_grad_, e.psf_width, fwid, fhei, FW_, FH_, transposed_};
         const int B = row_b_;
         const size_t rsm = row_buf_bytes(B, M_, sizeof(cx<T>), plan_m_.pad_shift);
-        set_smem(k_row_c2r<T, NT, Caps<T>::ROW, PsfWindowStore<T>, false>, rsm);
+        set_smem(k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PsfWindowStore<T>, false>, rsm);
         dim3 grid((unsigned)ceil_div(FH_, B), 1);
-        k_row_c2r<T, NT, Caps<T>::ROW, PsfWindowStore<T>, false><<<grid, NT, rsm, stream_>>>(
+        k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PsfWindowStore<T>, false><<<grid, RowNt<T>::value, rsm, stream_>>>(
             plan_m_, post_, SpecRef{xs, FH_, 0}, no_map_, FH_, FW_, B, FastDiv((uint32_t)B),
             (T)(1.0 / ((double)FW_ * (double)FH_)), epi, d_err_);
         UPDC_CUDA(cudaGetLastError());
@@ -966,17 +967,17 @@ template <typename T> class EngineImpl final : public Engine {
         for (const auto &rad : split_candidates(M)) {
             FftPlan plan;
             auto tab = fft_make_table<T>(M, rad, plan);
-            plan.pad_shift = fft_choose_padding(plan, NT, Caps<T>::ROW, std::max(1, std::min(2, Caps<T>::ROW / M)));
+            plan.pad_shift = fft_choose_padding(plan, RowNt<T>::value, Caps<T>::ROW, std::max(1, std::min(2, Caps<T>::ROW / M)));
             const size_t smem = row_buf_bytes(B, M, sizeof(cx<T>), plan.pad_shift);
             if (smem > SMEM_LIMIT) continue;
             cx<T> *dtab = dalloc<cx<T>>(tab.size(), nullptr);
             UPDC_CUDA(cudaMemcpy(dtab, tab.data(), tab.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
             plan.tw = dtab;
-            set_smem(k_row_r2c<T, NT, Caps<T>::ROW, PlaneLoader<T>, false>, smem);
+            set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false>, smem);
             const PlaneLoader<T> ld{plane, W_, 0};
             dim3 grid((unsigned)ceil_div(H_, B), 1);
             const float ms = time_launch([&] {
-                k_row_r2c<T, NT, Caps<T>::ROW, PlaneLoader<T>, false><<<grid, NT, smem, stream_>>>(
+                k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false><<<grid, RowNt<T>::value, smem, stream_>>>(
                     plan, dpost, ld, W_, H_, B, FastDiv((uint32_t)B), SpecRef{spec, H_, 0}, no_map_);
             });
             ++*timed;
@@ -1128,7 +1129,7 @@ template <typename T> class EngineImpl final : public Engine {
         // twiddle tables
         auto tm = fft_make_table<T>(M_, c.row_radices, plan_m_);
         auto th = fft_make_table<T>(FH_, c.col_radices, plan_h_);
-        plan_m_.pad_shift = fft_choose_padding(plan_m_, NT, Caps<T>::ROW, std::max(1, std::min(2, Caps<T>::ROW / M_)));
+        plan_m_.pad_shift = fft_choose_padding(plan_m_, RowNt<T>::value, Caps<T>::ROW, std::max(1, std::min(2, Caps<T>::ROW / M_)));
         plan_h_.pad_shift = fft_choose_padding(plan_h_, ColNt<T>::value, Caps<T>::COL_S, 1);
         cx<T> *dm = alloc<cx<T>>(tm.size()), *dh = alloc<cx<T>>(th.size());
         UPDC_CUDA(cudaMemcpy(dm, tm.data(), tm.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
@@ -1182,10 +1183,9 @@ template <typename T> class EngineImpl final : public Engine {
         row_b_ = std::max(1, std::min({Caps<T>::ROW / M_, TMA_UBOX / EW, ldh_}));
         if (EW == 1 && row_b_ >= 2) row_b_ &= ~1;
         // the FFT buffer and the staging tile share the block's shared memory
-        while (row_b_ > 2 && row_buf_bytes(row_b_, M_, sizeof(cx<T>), plan_m_.pad_shift) + row_stage_bytes(row_b_, M_, sizeof(cx<T>)) > SMEM_LIMIT)
+        while (row_b_ > 2 && row_tma_smem(row_b_, M_, sizeof(cx<T>), plan_m_.pad_shift) > SMEM_LIMIT)
             row_b_ -= EW == 1 ? 2 : 1;
-        use_tma_ = (row_b_ * EW) % 2 == 0 &&
-                   row_buf_bytes(row_b_, M_, sizeof(cx<T>), plan_m_.pad_shift) + row_stage_bytes(row_b_, M_, sizeof(cx<T>)) <= SMEM_LIMIT;
+        use_tma_ = (row_b_ * EW) % 2 == 0 && row_tma_smem(row_b_, M_, sizeof(cx<T>), plan_m_.pad_shift) <= SMEM_LIMIT;
         if (use_tma_) {
             const uint64_t d0 = (uint64_t)ldh_ * EW;
             const uint32_t ub = (uint32_t)row_ubox(M_);
@@ -1214,7 +1214,8 @@ template <typename T> class EngineImpl final : public Engine {
     CUtensorMap map_rx_{}, map_cr_{}, map_y_{}, map_rs_{}, no_map_{};
 
     size_t row_smem() const {
-        return row_buf_bytes(row_b_, M_, sizeof(cx<T>), plan_m_.pad_shift) + (use_tma_ ? row_stage_bytes(row_b_, M_, sizeof(cx<T>)) : 0);
+        return use_tma_ ? row_tma_smem(row_b_, M_, sizeof(cx<T>), plan_m_.pad_shift)
+                        : row_buf_bytes(row_b_, M_, sizeof(cx<T>), plan_m_.pad_shift);
     }
     int row_batch() const { return row_b_; }
     size_t fwd_smem() const {
@@ -1235,10 +1236,10 @@ template <typename T> class EngineImpl final : public Engine {
 
     void configure_kernels() {
         const size_t rs = row_smem();
-        set_smem(k_row_r2c<T, NT, Caps<T>::ROW, PlaneLoader<T>, true>, rs);
-        set_smem(k_row_r2c<T, NT, Caps<T>::ROW, PlaneLoader<T>, false>, rs);
-        set_smem(k_row_c2r<T, NT, Caps<T>::ROW, PlaneStore<T>, true>, rs);
-        set_smem(k_row_c2r<T, NT, Caps<T>::ROW, PlaneStore<T>, false>, rs);
+        set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, true>, rs);
+        set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false>, rs);
+        set_smem(k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, true>, rs);
+        set_smem(k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, false>, rs);
         const size_t fs = fwd_smem();
         set_smem(k_col_forward<T, ColNt<T>::value, Caps<T>::COL_S>, fs);
         set_smem(k_col_forward<T, ColNt<T>::value, Caps<T>::COL_L>, fs);
@@ -1268,10 +1269,10 @@ template <typename T> class EngineImpl final : public Engine {
         const PlaneLoader<T> ld{plane, W_, plane_stride};
         const SpecRef ref{out, ldh_, (size_t)(M_ + 1) * ldh_};
         if (use_tma_)
-            k_row_r2c<T, NT, Caps<T>::ROW, PlaneLoader<T>, true><<<grid, NT, row_smem(), stream_>>>(
+            k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, true><<<grid, RowNt<T>::value, row_smem(), stream_>>>(
                 plan_m_, post_, ld, W_, H_, B, FastDiv((uint32_t)B), ref, map);
         else
-            k_row_r2c<T, NT, Caps<T>::ROW, PlaneLoader<T>, false><<<grid, NT, row_smem(), stream_>>>(
+            k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false><<<grid, RowNt<T>::value, row_smem(), stream_>>>(
                 plan_m_, post_, ld, W_, H_, B, FastDiv((uint32_t)B), ref, no_map_);
         UPDC_CUDA(cudaGetLastError());
     }
@@ -1314,10 +1315,10 @@ template <typename T> class EngineImpl final : public Engine {
         const T scale = scale_factor();
         const SpecRef ref{const_cast<cx<T> *>(in), ldh_, (size_t)(M_ + 1) * ldh_};
         if (use_tma_)
-            k_row_c2r<T, NT, Caps<T>::ROW, PlaneStore<T>, true><<<grid, NT, row_smem(), stream_>>>(
+            k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, true><<<grid, RowNt<T>::value, row_smem(), stream_>>>(
                 plan_m_, post_, ref, map, H_, W_, B, FastDiv((uint32_t)B), scale, PlaneStore<T>{out, W_, nout_}, d_err_);
         else
-            k_row_c2r<T, NT, Caps<T>::ROW, PlaneStore<T>, false><<<grid, NT, row_smem(), stream_>>>(
+            k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, false><<<grid, RowNt<T>::value, row_smem(), stream_>>>(
                 plan_m_, post_, ref, no_map_, H_, W_, B, FastDiv((uint32_t)B), scale, PlaneStore<T>{out, W_, nout_}, d_err_);
         UPDC_CUDA(cudaGetLastError());
     }
@@ -1661,9 +1662,9 @@ template <typename T> class EngineImpl final : public Engine {
             PsfLoader<U, P> ld{dp, pw, transposed_ ? phh : pw, transposed_ ? pw : phh, FW_, FH_, transposed_, inv};
             const int B = Caps<U>::ROW / M_;
             const size_t rsm = row_buf_bytes(B, M_, sizeof(cx<U>), pm.pad_shift);
-            set_smem(k_row_r2c<U, NT, Caps<U>::ROW, PsfLoader<U, P>, false>, rsm);
+            set_smem(k_row_r2c<U, RowNt<U>::value, Caps<U>::ROW, PsfLoader<U, P>, false>, rsm);
             dim3 grid((unsigned)ceil_div(FH_, B), 1);
-            k_row_r2c<U, NT, Caps<U>::ROW, PsfLoader<U, P>, false><<<grid, NT, rsm, stream_>>>(
+            k_row_r2c<U, RowNt<U>::value, Caps<U>::ROW, PsfLoader<U, P>, false><<<grid, RowNt<U>::value, rsm, stream_>>>(
                 pm, post, ld, FW_, FH_, B, FastDiv((uint32_t)B), SpecRef{rp, FH_, 0}, no_map_);
             const size_t cs = fft_buf_bytes(FH_, sizeof(cx<U>), ph.pad_shift);
             if (FH_ <= Caps<U>::COL_S) {
@@ -1735,10 +1736,10 @@ template <typename T> class EngineImpl final : public Engine {
         cx<D> *rs = dalloc<cx<D>>(nexp_ * nu * H_, nullptr), *cr = dalloc<cx<D>>(nu * H_, nullptr);
         const int B = Caps<D>::ROW / M_;
         const size_t rsm = row_buf_bytes(B, M_, sizeof(cx<D>), pm.pad_shift);
-        set_smem(k_row_r2c<D, NT, Caps<D>::ROW, PlaneLoader<D>, false>, rsm);
+        set_smem(k_row_r2c<D, RowNt<D>::value, Caps<D>::ROW, PlaneLoader<D>, false>, rsm);
         {
             dim3 g((unsigned)ceil_div(H_, B), (unsigned)nexp_);
-            k_row_r2c<D, NT, Caps<D>::ROW, PlaneLoader<D>, false><<<g, NT, rsm, stream_>>>(
+            k_row_r2c<D, RowNt<D>::value, Caps<D>::ROW, PlaneLoader<D>, false><<<g, RowNt<D>::value, rsm, stream_>>>(
                 pm, dpost, PlaneLoader<D>{sc, W_, nout_}, W_, H_, B, FastDiv((uint32_t)B), SpecRef{rs, H_, nu * H_}, no_map_);
         }
         const size_t b = fft_buf_bytes(FH_, sizeof(cx<D>), ph.pad_shift);
@@ -1753,9 +1754,9 @@ template <typename T> class EngineImpl final : public Engine {
             k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_L><<<(unsigned)nu, NtAdj<D>::value, s, stream_>>>(ph, rs, H_, nu * H_, H_, kd, nu * FH_, nexp_, cr, H_, H_, aux);
         }
         D *den = dalloc<D>(nout_, nullptr);
-        set_smem(k_row_c2r<D, NT, Caps<D>::ROW, PlaneStore<D>, false>, rsm);
+        set_smem(k_row_c2r<D, RowNt<D>::value, Caps<D>::ROW, PlaneStore<D>, false>, rsm);
         dim3 g2((unsigned)ceil_div(H_, B), 1);
-        k_row_c2r<D, NT, Caps<D>::ROW, PlaneStore<D>, false><<<g2, NT, rsm, stream_>>>(
+        k_row_c2r<D, RowNt<D>::value, Caps<D>::ROW, PlaneStore<D>, false><<<g2, RowNt<D>::value, rsm, stream_>>>(
             pm, dpost, SpecRef{cr, H_, 0}, no_map_, H_, W_, B, FastDiv((uint32_t)B), 1.0 / (double)((size_t)FW_ * FH_),
             PlaneStore<D>{den, W_, 0}, d_err_);
         k_convert<D, T><<<grid1d(nout_), 256, 0, stream_>>>(den, den_, nout_);

@@ -32,6 +32,12 @@ constexpr size_t SPEC_SMEM_LIMIT = 227 * 1024;
 template <typename T> struct SpecColNt {
     static constexpr int value = sizeof(T) == 4 ? 384 : 512;
 };
+// Threads of the single-field engine's row kernels: 384 for FP32 (three
+// blocks per SM, which fit because the TMA tile is staged in the FFT
+// buffer's memory), 512 for FP64.
+template <typename T> struct SpecRowNt {
+    static constexpr int value = sizeof(T) == 4 ? 384 : 512;
+};
 // Shared-memory capacity (complex elements) of the FFT instantiations.
 template <typename T> struct SpecCaps {
     static constexpr int ROW = 5632;
@@ -102,6 +108,89 @@ __host__ __device__ inline size_t row_stage_bytes(int B, int M, size_t csize) {
     return (size_t)row_nbox(M) * row_ubox(M) * B * csize;
 }
 
+// ---------------------------------------------------------------------------- TMA tiles in place
+// With TMA the row kernels stage the block's u-major tile ({all bins} x {B
+// rows}, box by box) in the same shared memory as the FFT buffer: every
+// thread first reads what it needs into registers (its bin pairs u, M - u),
+// the block synchronises, and only then is the region overwritten in the
+// other layout.  Shared memory is the larger of the two layouts, not their
+// sum, so three blocks of 384 threads fit per SM.
+// Most bin pairs one thread holds: (M/2 + 1) * B <= CAP/2 + B with B <= 256.
+template <int CAP, int NT> struct RowPairs {
+    static constexpr int value = (CAP / 2 + 256 + NT - 1) / NT;
+};
+__host__ __device__ inline size_t row_tma_smem(int B, int M, size_t csize, int shift) {
+    const size_t a = row_buf_bytes(B, M, csize, shift), b = row_stage_bytes(B, M, csize);
+    return a > b ? a : b;
+}
+
+// Bin u of row b of the R2C output from the half-length FFT in buf.
+template <typename T>
+__device__ __forceinline__ cx<T> r2c_bin(const cx<T> *buf, int row0, int u, int M, int sh, const cx<T> *post) {
+    const T half = T(0.5);
+    const cx<T> Z = buf[fpad(row0 + (u == M ? 0 : u), sh)];
+    const cx<T> Zm = buf[fpad(row0 + (u == 0 ? 0 : M - u), sh)];
+    const cx<T> Zc = {Zm.x, -Zm.y};
+    const cx<T> E = {half * (Z.x + Zc.x), half * (Z.y + Zc.y)};
+    const cx<T> D = {half * (Z.x - Zc.x), half * (Z.y - Zc.y)};
+    const cx<T> P = fmulc(D, post[u]);
+    return {E.x + P.y, E.y - P.x};
+}
+
+template <typename T, int NT, int CAP>
+__device__ __forceinline__ void row_r2c_store_tma(cx<T> *buf, const cx<T> *__restrict__ post, int M, int sh, int B,
+                                                  int nb, FastDiv bdiv, const CUtensorMap *omap, int y0, int kexp) {
+    constexpr int KP = RowPairs<CAP, NT>::value;
+    const int npairs = (M / 2 + 1) * B;
+    cx<T> xa[KP], xb[KP];
+#pragma unroll
+    for (int j = 0; j < KP; ++j) {
+        const int q = threadIdx.x + j * NT;
+        xa[j] = xb[j] = cx<T>{T(0), T(0)};
+        if (q < npairs) {
+            const int u = (int)bdiv.div((uint32_t)q), b = q - u * B;
+            if (b < nb) {
+                xa[j] = r2c_bin(buf, b * M, u, M, sh, post);
+                xb[j] = r2c_bin(buf, b * M, M - u, M, sh, post);
+            }
+        }
+    }
+    __syncthreads();  // the FFT buffer is read; it becomes the staging tile
+    cx<T> *stage = buf;
+#pragma unroll
+    for (int j = 0; j < KP; ++j) {
+        const int q = threadIdx.x + j * NT;
+        if (q < npairs) {
+            const int u = (int)bdiv.div((uint32_t)q), b = q - u * B;
+            stage[u * B + b] = xa[j];
+            if (M - u != u) stage[(M - u) * B + b] = xb[j];
+        }
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        constexpr int EW = TmaElems<T>::value;
+        const int ub = row_ubox(M);
+        for (int bx = 0; bx < row_nbox(M); ++bx)
+            tma_store_3d(omap, stage + (size_t)bx * ub * B, y0 * EW, bx * ub, kexp);
+        tma_store_commit_and_wait();
+    }
+}
+
+// Inputs k and M - k of the C2R's half-length FFT from bins X[k], X[M-k].
+template <typename T>
+__device__ __forceinline__ cx<T> c2r_input(cx<T> X, cx<T> Xm, int k, const cx<T> *post) {
+    if (k == 0) {
+        X.y = 0;
+        Xm.y = 0;
+    }
+    const cx<T> S = {X.x + Xm.x, X.y - Xm.y};
+    const cx<T> D = {X.x - Xm.x, X.y + Xm.y};
+    const cx<T> w = post[k];
+    const cx<T> Q = fmulc_conj(D, w);
+    return {S.x - Q.y, S.y + Q.x};
+}
+
 // ---------------------------------------------------------------------------- row R2C
 // Rows [0, rows) of the real plane, zero-padded from W to FW = 2M columns,
 // transformed along x with an M-point complex FFT of z[m] = x[2m] + i x[2m+1]
@@ -128,7 +217,10 @@ __device__ __forceinline__ void row_r2c_tile(const FftPlan &plan, const cx<T> *_
         }
     __syncthreads();
     fft_batch<false, NT, CAP, FFT_RMAX>(buf, B, plan);
-    cx<T> *stage = reinterpret_cast<cx<T> *>(smem_raw + row_buf_bytes(B, M, sizeof(cx<T>), sh));
+    if constexpr (TMA) {
+        row_r2c_store_tma<T, NT, CAP>(buf, post, M, sh, B, nb, bdiv, omap, y0, kexp);
+        return;
+    }
     cx<T> *dst = reinterpret_cast<cx<T> *>(out.p) + kexp * out.batch_stride;
     const T half = T(0.5);
     for (int i = threadIdx.x; i < (M + 1) * B; i += NT) {
@@ -143,19 +235,7 @@ __device__ __forceinline__ void row_r2c_tile(const FftPlan &plan, const cx<T> *_
             const cx<T> P = fmulc(D, post[u]);
             X = {E.x + P.y, E.y - P.x};
         }
-        if (TMA) stage[i] = X;
-        else if (b < nb) dst[(size_t)u * out.ld + y0 + b] = X;
-    }
-    if (TMA) {
-        fence_proxy_async_smem();
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            constexpr int EW = TmaElems<T>::value;
-            const int ub = row_ubox(M);
-            for (int bx = 0; bx < row_nbox(M); ++bx)
-                tma_store_3d(omap, stage + (size_t)bx * ub * B, y0 * EW, bx * ub, kexp);
-            tma_store_commit_and_wait();
-        }
+        if (b < nb) dst[(size_t)u * out.ld + y0 + b] = X;
     }
 }
 
@@ -191,7 +271,7 @@ __device__ __forceinline__ void row_c2r_tile(const FftPlan &plan, const cx<T> *_
     __shared__ __align__(8) uint64_t bar;
     const int M = plan.n, sh = plan.pad_shift;
     const int nb = min(B, rows - y0);
-    cx<T> *stage = reinterpret_cast<cx<T> *>(smem_raw + row_buf_bytes(B, M, sizeof(cx<T>), sh));
+    cx<T> *stage = buf;  // TMA: the tile arrives in the FFT buffer's memory
     const cx<T> *src = reinterpret_cast<const cx<T> *>(in.p) + kexp * in.batch_stride;
     if (TMA) {
         if (threadIdx.x == 0) mbar_init(&bar, 1);
@@ -208,27 +288,41 @@ __device__ __forceinline__ void row_c2r_tile(const FftPlan &plan, const cx<T> *_
                 atomicMin(err, (unsigned long long)make_error_key(STAGE_UPDATE, blockIdx.x, ERR_DEVICE_TIMEOUT));
             return;
         }
-    }
-    for (int i = threadIdx.x; i < M * B; i += NT) {
-        const int k = (int)bdiv.div((uint32_t)i), b = i - k * B;
-        cx<T> Zp = {0, 0};
-        if (b < nb) {
-            cx<T> X, Xm;
-            if (TMA) {
-                X = stage[i];
-                Xm = stage[(M - k) * B + b];
-            } else {
-                X = src[(size_t)k * in.ld + y0 + b];
-                Xm = src[(size_t)(M - k) * in.ld + y0 + b];
+        // pairs (k, M - k): both inputs read into registers, then the tile's
+        // memory is overwritten with the FFT buffer
+        constexpr int KP = RowPairs<CAP, NT>::value;
+        const int npairs = (M / 2 + 1) * B;
+        cx<T> za[KP], zb[KP];
+#pragma unroll
+        for (int j = 0; j < KP; ++j) {
+            const int q = threadIdx.x + j * NT;
+            za[j] = zb[j] = cx<T>{T(0), T(0)};
+            if (q < npairs) {
+                const int k = (int)bdiv.div((uint32_t)q), b = q - k * B;
+                if (b < nb) {
+                    const cx<T> X = stage[k * B + b], Xm = stage[(M - k) * B + b];
+                    za[j] = c2r_input(X, Xm, k, post);
+                    if (k > 0) zb[j] = c2r_input(Xm, X, M - k, post);
+                }
             }
-            if (k == 0) { X.y = 0; Xm.y = 0; }
-            const cx<T> S = {X.x + Xm.x, X.y - Xm.y};
-            const cx<T> D = {X.x - Xm.x, X.y + Xm.y};
-            const cx<T> w = post[k];
-            const cx<T> Q = fmulc_conj(D, w);
-            Zp = {S.x - Q.y, S.y + Q.x};
         }
-        buf[fpad(b * M + k, sh)] = Zp;
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < KP; ++j) {
+            const int q = threadIdx.x + j * NT;
+            if (q < npairs) {
+                const int k = (int)bdiv.div((uint32_t)q), b = q - k * B;
+                buf[fpad(b * M + k, sh)] = za[j];
+                if (k > 0 && M - k != k) buf[fpad(b * M + M - k, sh)] = zb[j];
+            }
+        }
+    } else {
+        for (int i = threadIdx.x; i < M * B; i += NT) {
+            const int k = (int)bdiv.div((uint32_t)i), b = i - k * B;
+            cx<T> Zp = {0, 0};
+            if (b < nb) Zp = c2r_input(src[(size_t)k * in.ld + y0 + b], src[(size_t)(M - k) * in.ld + y0 + b], k, post);
+            buf[fpad(b * M + k, sh)] = Zp;
+        }
     }
     __syncthreads();
     fft_batch<true, NT, CAP, FFT_RMAX>(buf, B, plan);
