@@ -32,11 +32,12 @@ constexpr size_t SPEC_SMEM_LIMIT = 227 * 1024;
 template <typename T> struct SpecColNt {
     static constexpr int value = sizeof(T) == 4 ? 384 : 512;
 };
-// Threads of the single-field engine's row kernels: 384 for FP32 (three
+// Threads of the single-field engine's row kernels: 256 for FP32 (four
 // blocks per SM, which fit because the TMA tile is staged in the FFT
-// buffer's memory), 512 for FP64.
+// buffer's memory; measured on c1 against 384 x 3 and 512 x 2: 6.44, 6.53
+// and 6.69 ms per iteration), 512 for FP64.
 template <typename T> struct SpecRowNt {
-    static constexpr int value = sizeof(T) == 4 ? 384 : 512;
+    static constexpr int value = sizeof(T) == 4 ? 256 : 512;
 };
 // Shared-memory capacity (complex elements) of the FFT instantiations.
 template <typename T> struct SpecCaps {
