@@ -254,8 +254,8 @@ template <typename T> class BatchImpl final : public Batch {
         build_units();
         if (smem_row_ > SPEC_SMEM_LIMIT || smem_fwd_ > SPEC_SMEM_LIMIT || smem_adj_ > SPEC_SMEM_LIMIT)
             throw Error(1, "batched transforms exceed the shared-memory limit");
-        set_attr(kb_row_r2c<T, SPEC_NT, SpecCaps<T>::ROW>, smem_row_);
-        set_attr(kb_row_c2r<T, SPEC_NT, SpecCaps<T>::ROW>, smem_row_);
+        set_attr(kb_row_r2c<T, SpecRowNt<T>::value, SpecCaps<T>::ROW>, smem_row_);
+        set_attr(kb_row_c2r<T, SpecRowNt<T>::value, SpecCaps<T>::ROW>, smem_row_);
         set_attr(kb_col_forward<T, SPEC_NT, SpecCaps<T>::COL_S>, smem_fwd_);
         if constexpr (sizeof(T) == 4) {
             set_attr(kb_col_adjoint<T, AccF64, SpecNtAdj<T>::value, SpecCaps<T>::COL_S>, smem_adj_);
@@ -377,20 +377,20 @@ template <typename T> class BatchImpl final : public Batch {
 
     void enqueue_iteration() {
         const int nf = (int)host_.size();
-        constexpr int NT = SPEC_NT;
+        constexpr int NT = SPEC_NT, RNT = SpecRowNt<T>::value;
         constexpr int ROW = SpecCaps<T>::ROW, COL = SpecCaps<T>::COL_S;
         kb_reset<T><<<nf, 32, 0, stream_>>>(d_fields_);
-        kb_row_r2c<T, NT, ROW><<<grid_for(nunits_[0]), NT, smem_row_, stream_>>>(d_fields_, d_units_[0], (int)nunits_[0], 0);
+        kb_row_r2c<T, RNT, ROW><<<grid_for(nunits_[0]), RNT, smem_row_, stream_>>>(d_fields_, d_units_[0], (int)nunits_[0], 0);
         kb_col_forward<T, NT, COL><<<grid_for(nunits_[1]), NT, smem_fwd_, stream_>>>(d_fields_, d_units_[1], (int)nunits_[1]);
-        kb_row_c2r<T, NT, ROW><<<grid_for(nunits_[2]), NT, smem_row_, stream_>>>(d_fields_, d_units_[2], (int)nunits_[2], 0);
+        kb_row_c2r<T, RNT, ROW><<<grid_for(nunits_[2]), RNT, smem_row_, stream_>>>(d_fields_, d_units_[2], (int)nunits_[2], 0);
         if (comp_mu_)
             kb_detector<T, true><<<grid_for(nunits_[3]), DET_WARPS * 32, 0, stream_>>>(d_fields_, d_units_[3], (int)nunits_[3]);
         else
             kb_detector<T, false><<<grid_for(nunits_[3]), DET_WARPS * 32, 0, stream_>>>(d_fields_, d_units_[3], (int)nunits_[3]);
         kb_scatter<T><<<grid_for(nunits_[4]), 256, 0, stream_>>>(d_fields_, d_units_[4], (int)nunits_[4]);
-        kb_row_r2c<T, NT, ROW><<<grid_for(nunits_[5]), NT, smem_row_, stream_>>>(d_fields_, d_units_[5], (int)nunits_[5], 1);
+        kb_row_r2c<T, RNT, ROW><<<grid_for(nunits_[5]), RNT, smem_row_, stream_>>>(d_fields_, d_units_[5], (int)nunits_[5], 1);
         launch_adjoint();
-        kb_row_c2r<T, NT, ROW><<<grid_for(nunits_[7]), NT, smem_row_, stream_>>>(d_fields_, d_units_[7], (int)nunits_[7], 1);
+        kb_row_c2r<T, RNT, ROW><<<grid_for(nunits_[7]), RNT, smem_row_, stream_>>>(d_fields_, d_units_[7], (int)nunits_[7], 1);
         kb_update<T><<<grid_for(nunits_[6]), 256, 0, stream_>>>(d_fields_, d_units_[6], (int)nunits_[6]);
         kb_reduce<T><<<nf, 256, 0, stream_>>>(d_fields_);
         UPDC_CUDA(cudaGetLastError());
