@@ -86,12 +86,19 @@ template <typename T> struct LinkSum {
 // raw_mu.
 // Block `block` of `nblocks` over exposure k's pixels (grid-stride); the
 // body of k_detector and of the batched detector (batch.cuh).
-template <typename T, bool COMP>
-__device__ __forceinline__ void detector_tiles(const ExpDesc<T> &e, int k, size_t nin, const T *__restrict__ blur,
-                                               T *__restrict__ wr, ExpStats *__restrict__ stats,
-                                               unsigned long long *__restrict__ err, unsigned block, unsigned nblocks) {
-    __shared__ uint32_t s_idx[DET_WARPS][DET_LCAP];
-    __shared__ float s_frac[DET_WARPS][DET_LCAP];
+struct DetShared {
+    uint32_t idx[DET_WARPS][DET_LCAP];
+    float frac[DET_WARPS][DET_LCAP];
+    unsigned long long nnew[DET_WARPS], ntot[DET_WARPS], mn[DET_WARPS];
+};
+
+template <typename T, bool COMP, bool DELTA16>
+__device__ __forceinline__ void detector_tiles_enc(const ExpDesc<T> &e, int k, size_t nin, const T *__restrict__ blur,
+                                                   T *__restrict__ wr, ExpStats *__restrict__ stats,
+                                                   unsigned long long *__restrict__ err, unsigned block,
+                                                   unsigned nblocks, DetShared &sh) {
+    auto &s_idx = sh.idx;
+    auto &s_frac = sh.frac;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned long long nnew = 0, ntot = 0, mn = ~0ull;
     const size_t step = (size_t)nblocks * DET_WARPS * 32;
@@ -101,7 +108,7 @@ __device__ __forceinline__ void detector_tiles(const ExpDesc<T> &e, int k, size_
         // every per-pixel load first (independent of each other)
         const uint32_t z0 = valid ? e.off[p] : 0u, z1 = valid ? e.off[p + 1] : 0u;
         const T w = valid ? e.wht[p] : T(0);
-        const uint32_t bse = (valid && e.delta16) ? e.base[p] : 0u;
+        const uint32_t bse = (valid && DELTA16) ? e.base[p] : 0u;
         const T sci = valid ? e.sci[p] : T(0);
         uint8_t fz = valid ? e.frozen[p] : (uint8_t)0;
         const int last = (int)min((size_t)31, nin - 1 - p0);
@@ -118,7 +125,7 @@ __device__ __forceinline__ void detector_tiles(const ExpDesc<T> &e, int k, size_
             for (int j = 0; j < NS; ++j) {
                 const uint32_t i = lane + 32u * j;
                 fv[j] = i < cnt ? e.frac[zb + i] : 0.0f;
-                iv[j] = i < cnt ? (e.delta16 ? (uint32_t)e.delta[zb + i] : e.tgt[zb + i]) : 0u;
+                iv[j] = i < cnt ? (DELTA16 ? (uint32_t)e.delta[zb + i] : e.tgt[zb + i]) : 0u;
             }
 #pragma unroll
             for (int j = 0; j < NS; ++j) {
@@ -153,7 +160,7 @@ __device__ __forceinline__ void detector_tiles(const ExpDesc<T> &e, int k, size_
                     }
                 } else {
                     for (uint32_t z = z0; z < z1; ++z) {
-                        const uint32_t t = e.delta16 ? bse + (uint32_t)e.delta[z] : e.tgt[z];
+                        const uint32_t t = DELTA16 ? bse + (uint32_t)e.delta[z] : e.tgt[z];
                         acc.template add<COMP>(e.frac[z], blur[t]);
                     }
                 }
@@ -185,7 +192,9 @@ __device__ __forceinline__ void detector_tiles(const ExpDesc<T> &e, int k, size_
         __syncwarp();  // the next tile reuses this warp's staging area
     }
     // block reduction of the counters
-    __shared__ unsigned long long s_new[DET_WARPS], s_tot[DET_WARPS], s_min[DET_WARPS];
+    auto &s_new = sh.nnew;
+    auto &s_tot = sh.ntot;
+    auto &s_min = sh.mn;
     nnew = block_sum_warp(nnew);
     ntot = block_sum_warp(ntot);
     mn = warp_min_u64(mn);
@@ -210,6 +219,17 @@ __device__ __forceinline__ void detector_tiles(const ExpDesc<T> &e, int k, size_
 
 // Four 256-thread blocks per SM (64 registers; measured 5% faster than three
 // blocks at 80 registers on B200).
+// The exposure's LinkMap encoding is fixed per exposure; each block takes
+// the instantiation of its encoding (a block-uniform branch).
+template <typename T, bool COMP>
+__device__ __forceinline__ void detector_tiles(const ExpDesc<T> &e, int k, size_t nin, const T *__restrict__ blur,
+                                               T *__restrict__ wr, ExpStats *__restrict__ stats,
+                                               unsigned long long *__restrict__ err, unsigned block, unsigned nblocks) {
+    __shared__ DetShared sh;
+    if (e.delta16) detector_tiles_enc<T, COMP, true>(e, k, nin, blur, wr, stats, err, block, nblocks, sh);
+    else detector_tiles_enc<T, COMP, false>(e, k, nin, blur, wr, stats, err, block, nblocks, sh);
+}
+
 template <typename T, bool COMP>
 __global__ void __launch_bounds__(DET_WARPS * 32, 4) k_detector(const ExpDesc<T> *__restrict__ exps, size_t nin, size_t nout,
                                                            const T *__restrict__ blur_all, T *__restrict__ wr_all,
