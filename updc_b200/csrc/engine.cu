@@ -237,6 +237,8 @@ constexpr int NT = SPEC_NT;
 template <typename T> using NtAdj = SpecNtAdj<T>;
 template <typename T> using ColNt = SpecColNt<T>;
 template <typename T> using RowNt = SpecRowNt<T>;
+// FP32 column kernels always keep X-hat and the accumulator in global scratch
+template <typename T> constexpr int ColAux = sizeof(T) == 4 ? 1 : 0;
 template <typename T> using Caps = SpecCaps<T>;
 constexpr size_t SMEM_LIMIT = SPEC_SMEM_LIMIT;
 
@@ -1241,8 +1243,8 @@ template <typename T> class EngineImpl final : public Engine {
         set_smem(k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, true>, rs);
         set_smem(k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, false>, rs);
         const size_t fs = fwd_smem();
-        set_smem(k_col_forward<T, ColNt<T>::value, Caps<T>::COL_S>, fs);
-        set_smem(k_col_forward<T, ColNt<T>::value, Caps<T>::COL_L>, fs);
+        set_smem(k_col_forward<T, ColNt<T>::value, Caps<T>::COL_S, ColAux<T>>, fs);
+        set_smem(k_col_forward<T, ColNt<T>::value, Caps<T>::COL_L, ColAux<T>>, fs);
         set_smem(k_col_fft<T, NT, Caps<T>::COL_S, false>, fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift));
         set_smem(k_col_fft<T, NT, Caps<T>::COL_L, false>, fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift));
         configure_adjoint<AccPlain<T>>();
@@ -1255,8 +1257,8 @@ template <typename T> class EngineImpl final : public Engine {
         if constexpr (sizeof(typename Acc::S) > 0) {
             if constexpr (std::is_same<Acc, AccPlain<T>>::value || sizeof(T) == 4) {
                 const size_t s = adj_smem<Acc>();
-                set_smem(k_col_adjoint<T, Acc, ColNt<T>::value, Caps<T>::COL_S>, s);
-                set_smem(k_col_adjoint<T, Acc, ColNt<T>::value, Caps<T>::COL_L>, s);
+                set_smem(k_col_adjoint<T, Acc, ColNt<T>::value, Caps<T>::COL_S, ColAux<T>>, s);
+                set_smem(k_col_adjoint<T, Acc, ColNt<T>::value, Caps<T>::COL_L, ColAux<T>>, s);
             }
         }
     }
@@ -1280,9 +1282,9 @@ template <typename T> class EngineImpl final : public Engine {
         const size_t nu = (size_t)M_ + 1;
         const size_t ks = nu * FH_, ys = nu * ldh_;
         if (FH_ <= Caps<T>::COL_S)
-            k_col_forward<T, ColNt<T>::value, Caps<T>::COL_S><<<(unsigned)nu, ColNt<T>::value, fwd_smem(), stream_>>>(plan_h_, rx_, ldh_, H_, khat_ + act_k0_ * ks, ks, act_n_, act_y(), ldh_, ys, H_, (int)nu, aux_fwd_);
+            k_col_forward<T, ColNt<T>::value, Caps<T>::COL_S, ColAux<T>><<<(unsigned)nu, ColNt<T>::value, fwd_smem(), stream_>>>(plan_h_, rx_, ldh_, H_, khat_ + act_k0_ * ks, ks, act_n_, act_y(), ldh_, ys, H_, (int)nu, aux_fwd_);
         else
-            k_col_forward<T, ColNt<T>::value, Caps<T>::COL_L><<<(unsigned)nu, ColNt<T>::value, fwd_smem(), stream_>>>(plan_h_, rx_, ldh_, H_, khat_ + act_k0_ * ks, ks, act_n_, act_y(), ldh_, ys, H_, (int)nu, aux_fwd_);
+            k_col_forward<T, ColNt<T>::value, Caps<T>::COL_L, ColAux<T>><<<(unsigned)nu, ColNt<T>::value, fwd_smem(), stream_>>>(plan_h_, rx_, ldh_, H_, khat_ + act_k0_ * ks, ks, act_n_, act_y(), ldh_, ys, H_, (int)nu, aux_fwd_);
         UPDC_CUDA(cudaGetLastError());
     }
     template <class Acc> void ensure_adj_aux() {
@@ -1297,9 +1299,9 @@ template <typename T> class EngineImpl final : public Engine {
         }
         const size_t s = adj_smem<Acc>();
         if (FH_ <= Caps<T>::COL_S)
-            k_col_adjoint<T, Acc, ColNt<T>::value, Caps<T>::COL_S><<<(unsigned)nu, ColNt<T>::value, s, stream_>>>(plan_h_, act_rs(), ldh_, nu * ldh_, H_, khat + act_k0_ * nu * FH_, nu * FH_, act_n_, cr_, ldh_, H_, aux);
+            k_col_adjoint<T, Acc, ColNt<T>::value, Caps<T>::COL_S, ColAux<T>><<<(unsigned)nu, ColNt<T>::value, s, stream_>>>(plan_h_, act_rs(), ldh_, nu * ldh_, H_, khat + act_k0_ * nu * FH_, nu * FH_, act_n_, cr_, ldh_, H_, aux);
         else
-            k_col_adjoint<T, Acc, ColNt<T>::value, Caps<T>::COL_L><<<(unsigned)nu, ColNt<T>::value, s, stream_>>>(plan_h_, act_rs(), ldh_, nu * ldh_, H_, khat + act_k0_ * nu * FH_, nu * FH_, act_n_, cr_, ldh_, H_, aux);
+            k_col_adjoint<T, Acc, ColNt<T>::value, Caps<T>::COL_L, ColAux<T>><<<(unsigned)nu, ColNt<T>::value, s, stream_>>>(plan_h_, act_rs(), ldh_, nu * ldh_, H_, khat + act_k0_ * nu * FH_, nu * FH_, act_n_, cr_, ldh_, H_, aux);
         UPDC_CUDA(cudaGetLastError());
     }
     void launch_col_adjoint() {

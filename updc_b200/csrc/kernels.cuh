@@ -362,14 +362,19 @@ __device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes) {
     if (e > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((uint32_t)(e - a)) : "memory");
 }
 
-template <typename T, int NT, int CAP>
+// AUX = 1: the caller guarantees `aux` (global scratch) is given, so its
+// accesses compile to global loads and stores; AUX = 0 decides at run time
+// between `aux` and shared memory (generic accesses).
+template <typename T, int NT, int CAP, int AUX = 0>
 __device__ __forceinline__ void col_forward_column(const FftPlan &plan, const cx<T> *__restrict__ rx, int ldr,
                                                    int rows_in, const cx<T> *__restrict__ khat, size_t khat_stride,
                                                    int nexp, cx<T> *__restrict__ y, int ldy, size_t y_stride,
                                                    int rows_out, cx<T> *aux, int u, unsigned char *smem_raw) {
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
     const int n = plan.n, sh = plan.pad_shift;
-    cx<T> *xh = aux ? aux + (size_t)u * n : reinterpret_cast<cx<T> *>(smem_raw + fft_buf_bytes(n, sizeof(cx<T>), sh));
+    cx<T> *xh;
+    if constexpr (AUX == 1) xh = aux + (size_t)u * n;
+    else xh = aux ? aux + (size_t)u * n : reinterpret_cast<cx<T> *>(smem_raw + fft_buf_bytes(n, sizeof(cx<T>), sh));
     const cx<T> *src = rx + (size_t)u * ldr;
 #pragma unroll 1
     for (int it = 0; it <= nexp; ++it) {
@@ -399,15 +404,15 @@ __device__ __forceinline__ void col_forward_column(const FftPlan &plan, const cx
     }
 }
 
-template <typename T, int NT, int CAP>
+template <typename T, int NT, int CAP, int AUX = 0>
 __global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_forward(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ rx, int ldr, int rows_in,
                                                     const cx<T> *__restrict__ khat, size_t khat_stride, int nexp,
                                                     cx<T> *__restrict__ y, int ldy, size_t y_stride, int rows_out,
                                                     int nu, cx<T> *aux) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     (void)nu;
-    col_forward_column<T, NT, CAP>(plan, rx, ldr, rows_in, khat, khat_stride, nexp, y, ldy, y_stride, rows_out, aux,
-                                   blockIdx.x, smem_raw);
+    col_forward_column<T, NT, CAP, AUX>(plan, rx, ldr, rows_in, khat, khat_stride, nexp, y, ldy, y_stride, rows_out,
+                                        aux, blockIdx.x, smem_raw);
 }
 
 // Cross-exposure accumulation policies for the adjoint sum
@@ -455,15 +460,17 @@ struct AccKahan {  // FP32 products, Kahan-compensated FP32 sum
 // for y < rows_out.  The sum over k runs in exposure order inside the block;
 // the final inverse goes through the same forward-FFT call site as
 // conj(FFT(conj(.))).
-template <typename T, class Acc, int NT, int CAP>
+template <typename T, class Acc, int NT, int CAP, int AUX = 0>
 __device__ __forceinline__ void col_adjoint_column(const FftPlan &plan, const cx<T> *__restrict__ rs, int ldr,
                                                    size_t rs_stride, int rows_in, const cx<T> *__restrict__ khat,
                                                    size_t khat_stride, int nexp, cx<T> *__restrict__ c, int ldc,
                                                    int rows_out, typename Acc::S *aux, int u, unsigned char *smem_raw) {
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
     const int n = plan.n, sh = plan.pad_shift;
-    typename Acc::S *acc = aux ? aux + (size_t)u * n
-                               : reinterpret_cast<typename Acc::S *>(smem_raw + fft_buf_bytes(n, sizeof(cx<T>), sh));
+    typename Acc::S *acc;
+    if constexpr (AUX == 1) acc = aux + (size_t)u * n;
+    else acc = aux ? aux + (size_t)u * n
+                   : reinterpret_cast<typename Acc::S *>(smem_raw + fft_buf_bytes(n, sizeof(cx<T>), sh));
     for (int v = threadIdx.x; v < n; v += NT) Acc::zero(acc[v]);
 #pragma unroll 1
     for (int it = 0; it <= nexp; ++it) {
@@ -492,13 +499,13 @@ __device__ __forceinline__ void col_adjoint_column(const FftPlan &plan, const cx
     }
 }
 
-template <typename T, class Acc, int NT, int CAP>
+template <typename T, class Acc, int NT, int CAP, int AUX = 0>
 __global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_adjoint(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ rs, int ldr, size_t rs_stride,
                                                     int rows_in, const cx<T> *__restrict__ khat, size_t khat_stride, int nexp,
                                                     cx<T> *__restrict__ c, int ldc, int rows_out, typename Acc::S *aux) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    col_adjoint_column<T, Acc, NT, CAP>(plan, rs, ldr, rs_stride, rows_in, khat, khat_stride, nexp, c, ldc, rows_out,
-                                        aux, blockIdx.x, smem_raw);
+    col_adjoint_column<T, Acc, NT, CAP, AUX>(plan, rs, ldr, rs_stride, rows_in, khat, khat_stride, nexp, c, ldc,
+                                             rows_out, aux, blockIdx.x, smem_raw);
 }
 
 // Plain column transform (setup: PSF spectra and generic 2-D transforms).
