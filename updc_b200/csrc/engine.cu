@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <functional>
+#include <type_traits>
 #include <map>
 #include <unistd.h>
 #include <chrono>
@@ -239,6 +240,13 @@ template <typename T> using ColNt = SpecColNt<T>;
 template <typename T> using RowNt = SpecRowNt<T>;
 // FP32 column kernels always keep X-hat and the accumulator in global scratch
 template <typename T> constexpr int ColAux = sizeof(T) == 4 ? 1 : 0;
+// Runs f with the plan's padding shift as a compile-time constant where the
+// kernels are compiled for it (31: no padding, every fpad() folds away),
+// else with -1 (the kernels read it from the plan).
+template <class F> void by_pad(int sh, F &&f) {
+    if (sh == 31) f(std::integral_constant<int, 31>{});
+    else f(std::integral_constant<int, -1>{});
+}
 template <typename T> using Caps = SpecCaps<T>;
 constexpr size_t SMEM_LIMIT = SPEC_SMEM_LIMIT;
 
@@ -975,12 +983,17 @@ template <typename T> class EngineImpl final : public Engine {
             cx<T> *dtab = dalloc<cx<T>>(tab.size(), nullptr);
             UPDC_CUDA(cudaMemcpy(dtab, tab.data(), tab.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
             plan.tw = dtab;
-            set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false>, smem);
             const PlaneLoader<T> ld{plane, W_, 0};
             dim3 grid((unsigned)ceil_div(H_, B), 1);
-            const float ms = time_launch([&] {
-                k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false><<<grid, RowNt<T>::value, smem, stream_>>>(
-                    plan, dpost, ld, W_, H_, B, FastDiv((uint32_t)B), SpecRef{spec, H_, 0}, no_map_);
+            float ms = 0;
+            by_pad(plan.pad_shift, [&](auto P) {
+                constexpr int PS = decltype(P)::value;
+                set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false, PS>, smem);
+                ms = time_launch([&] {
+                    k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false, PS>
+                        <<<grid, RowNt<T>::value, smem, stream_>>>(plan, dpost, ld, W_, H_, B, FastDiv((uint32_t)B),
+                                                                   SpecRef{spec, H_, 0}, no_map_);
+                });
             });
             ++*timed;
             cudaFree(dtab);
@@ -1003,19 +1016,22 @@ template <typename T> class EngineImpl final : public Engine {
             cx<T> *dtab = dalloc<cx<T>>(tab.size(), nullptr);
             UPDC_CUDA(cudaMemcpy(dtab, tab.data(), tab.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
             plan.tw = dtab;
-            float ms;
+            float ms = 0;
             constexpr int CNT = ColNt<T>::value;
-            if (FH <= Caps<T>::COL_S) {
-                set_smem(k_col_fft<T, CNT, Caps<T>::COL_S, false>, smem);
-                ms = time_launch([&] {
-                    k_col_fft<T, CNT, Caps<T>::COL_S, false><<<(unsigned)nc, CNT, smem, stream_>>>(plan, in, H_, H_, out, FH, FH);
-                });
-            } else {
-                set_smem(k_col_fft<T, CNT, Caps<T>::COL_L, false>, smem);
-                ms = time_launch([&] {
-                    k_col_fft<T, CNT, Caps<T>::COL_L, false><<<(unsigned)nc, CNT, smem, stream_>>>(plan, in, H_, H_, out, FH, FH);
-                });
-            }
+            by_pad(plan.pad_shift, [&](auto P) {
+                constexpr int PS = decltype(P)::value;
+                if (FH <= Caps<T>::COL_S) {
+                    set_smem(k_col_fft<T, CNT, Caps<T>::COL_S, false, PS>, smem);
+                    ms = time_launch([&] {
+                        k_col_fft<T, CNT, Caps<T>::COL_S, false, PS><<<(unsigned)nc, CNT, smem, stream_>>>(plan, in, H_, H_, out, FH, FH);
+                    });
+                } else {
+                    set_smem(k_col_fft<T, CNT, Caps<T>::COL_L, false, PS>, smem);
+                    ms = time_launch([&] {
+                        k_col_fft<T, CNT, Caps<T>::COL_L, false, PS><<<(unsigned)nc, CNT, smem, stream_>>>(plan, in, H_, H_, out, FH, FH);
+                    });
+                }
+            });
             ++*timed;
             cudaFree(dtab);
             if (ms / nc < best.second) best = {rad, ms / nc};
@@ -1238,13 +1254,19 @@ template <typename T> class EngineImpl final : public Engine {
 
     void configure_kernels() {
         const size_t rs = row_smem();
-        set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, true>, rs);
-        set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false>, rs);
-        set_smem(k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, true>, rs);
-        set_smem(k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, false>, rs);
+        by_pad(plan_m_.pad_shift, [&](auto P) {
+            constexpr int PS = decltype(P)::value;
+            set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, true, PS>, rs);
+            set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false, PS>, rs);
+            set_smem(k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, true, PS>, rs);
+            set_smem(k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, false, PS>, rs);
+        });
         const size_t fs = fwd_smem();
-        set_smem(k_col_forward<T, ColNt<T>::value, Caps<T>::COL_S, ColAux<T>>, fs);
-        set_smem(k_col_forward<T, ColNt<T>::value, Caps<T>::COL_L, ColAux<T>>, fs);
+        by_pad(plan_h_.pad_shift, [&](auto P) {
+            constexpr int PS = decltype(P)::value;
+            set_smem(k_col_forward<T, ColNt<T>::value, Caps<T>::COL_S, ColAux<T>, PS>, fs);
+            set_smem(k_col_forward<T, ColNt<T>::value, Caps<T>::COL_L, ColAux<T>, PS>, fs);
+        });
         set_smem(k_col_fft<T, NT, Caps<T>::COL_S, false>, fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift));
         set_smem(k_col_fft<T, NT, Caps<T>::COL_L, false>, fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift));
         configure_adjoint<AccPlain<T>>();
@@ -1257,8 +1279,11 @@ template <typename T> class EngineImpl final : public Engine {
         if constexpr (sizeof(typename Acc::S) > 0) {
             if constexpr (std::is_same<Acc, AccPlain<T>>::value || sizeof(T) == 4) {
                 const size_t s = adj_smem<Acc>();
-                set_smem(k_col_adjoint<T, Acc, ColNt<T>::value, Caps<T>::COL_S, ColAux<T>>, s);
-                set_smem(k_col_adjoint<T, Acc, ColNt<T>::value, Caps<T>::COL_L, ColAux<T>>, s);
+                by_pad(plan_h_.pad_shift, [&](auto P) {
+                    constexpr int PS = decltype(P)::value;
+                    set_smem(k_col_adjoint<T, Acc, ColNt<T>::value, Caps<T>::COL_S, ColAux<T>, PS>, s);
+                    set_smem(k_col_adjoint<T, Acc, ColNt<T>::value, Caps<T>::COL_L, ColAux<T>, PS>, s);
+                });
             }
         }
     }
@@ -1270,21 +1295,27 @@ template <typename T> class EngineImpl final : public Engine {
         dim3 grid((unsigned)ceil_div(H_, B), (unsigned)batch);
         const PlaneLoader<T> ld{plane, W_, plane_stride};
         const SpecRef ref{out, ldh_, (size_t)(M_ + 1) * ldh_};
-        if (use_tma_)
-            k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, true><<<grid, RowNt<T>::value, row_smem(), stream_>>>(
-                plan_m_, post_, ld, W_, H_, B, FastDiv((uint32_t)B), ref, map);
-        else
-            k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false><<<grid, RowNt<T>::value, row_smem(), stream_>>>(
-                plan_m_, post_, ld, W_, H_, B, FastDiv((uint32_t)B), ref, no_map_);
+        by_pad(plan_m_.pad_shift, [&](auto P) {
+            constexpr int PS = decltype(P)::value;
+            if (use_tma_)
+                k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, true, PS><<<grid, RowNt<T>::value, row_smem(), stream_>>>(
+                    plan_m_, post_, ld, W_, H_, B, FastDiv((uint32_t)B), ref, map);
+            else
+                k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false, PS><<<grid, RowNt<T>::value, row_smem(), stream_>>>(
+                    plan_m_, post_, ld, W_, H_, B, FastDiv((uint32_t)B), ref, no_map_);
+        });
         UPDC_CUDA(cudaGetLastError());
     }
     void launch_col_forward() {
         const size_t nu = (size_t)M_ + 1;
         const size_t ks = nu * FH_, ys = nu * ldh_;
-        if (FH_ <= Caps<T>::COL_S)
-            k_col_forward<T, ColNt<T>::value, Caps<T>::COL_S, ColAux<T>><<<(unsigned)nu, ColNt<T>::value, fwd_smem(), stream_>>>(plan_h_, rx_, ldh_, H_, khat_ + act_k0_ * ks, ks, act_n_, act_y(), ldh_, ys, H_, (int)nu, aux_fwd_);
-        else
-            k_col_forward<T, ColNt<T>::value, Caps<T>::COL_L, ColAux<T>><<<(unsigned)nu, ColNt<T>::value, fwd_smem(), stream_>>>(plan_h_, rx_, ldh_, H_, khat_ + act_k0_ * ks, ks, act_n_, act_y(), ldh_, ys, H_, (int)nu, aux_fwd_);
+        by_pad(plan_h_.pad_shift, [&](auto P) {
+            constexpr int PS = decltype(P)::value;
+            if (FH_ <= Caps<T>::COL_S)
+                k_col_forward<T, ColNt<T>::value, Caps<T>::COL_S, ColAux<T>, PS><<<(unsigned)nu, ColNt<T>::value, fwd_smem(), stream_>>>(plan_h_, rx_, ldh_, H_, khat_ + act_k0_ * ks, ks, act_n_, act_y(), ldh_, ys, H_, (int)nu, aux_fwd_);
+            else
+                k_col_forward<T, ColNt<T>::value, Caps<T>::COL_L, ColAux<T>, PS><<<(unsigned)nu, ColNt<T>::value, fwd_smem(), stream_>>>(plan_h_, rx_, ldh_, H_, khat_ + act_k0_ * ks, ks, act_n_, act_y(), ldh_, ys, H_, (int)nu, aux_fwd_);
+        });
         UPDC_CUDA(cudaGetLastError());
     }
     template <class Acc> void ensure_adj_aux() {
@@ -1298,10 +1329,13 @@ template <typename T> class EngineImpl final : public Engine {
             aux = (typename Acc::S *)aux_adj_;
         }
         const size_t s = adj_smem<Acc>();
-        if (FH_ <= Caps<T>::COL_S)
-            k_col_adjoint<T, Acc, ColNt<T>::value, Caps<T>::COL_S, ColAux<T>><<<(unsigned)nu, ColNt<T>::value, s, stream_>>>(plan_h_, act_rs(), ldh_, nu * ldh_, H_, khat + act_k0_ * nu * FH_, nu * FH_, act_n_, cr_, ldh_, H_, aux);
-        else
-            k_col_adjoint<T, Acc, ColNt<T>::value, Caps<T>::COL_L, ColAux<T>><<<(unsigned)nu, ColNt<T>::value, s, stream_>>>(plan_h_, act_rs(), ldh_, nu * ldh_, H_, khat + act_k0_ * nu * FH_, nu * FH_, act_n_, cr_, ldh_, H_, aux);
+        by_pad(plan_h_.pad_shift, [&](auto P) {
+            constexpr int PS = decltype(P)::value;
+            if (FH_ <= Caps<T>::COL_S)
+                k_col_adjoint<T, Acc, ColNt<T>::value, Caps<T>::COL_S, ColAux<T>, PS><<<(unsigned)nu, ColNt<T>::value, s, stream_>>>(plan_h_, act_rs(), ldh_, nu * ldh_, H_, khat + act_k0_ * nu * FH_, nu * FH_, act_n_, cr_, ldh_, H_, aux);
+            else
+                k_col_adjoint<T, Acc, ColNt<T>::value, Caps<T>::COL_L, ColAux<T>, PS><<<(unsigned)nu, ColNt<T>::value, s, stream_>>>(plan_h_, act_rs(), ldh_, nu * ldh_, H_, khat + act_k0_ * nu * FH_, nu * FH_, act_n_, cr_, ldh_, H_, aux);
+        });
         UPDC_CUDA(cudaGetLastError());
     }
     void launch_col_adjoint() {
@@ -1316,12 +1350,15 @@ template <typename T> class EngineImpl final : public Engine {
         dim3 grid((unsigned)ceil_div(H_, B), (unsigned)batch);
         const T scale = scale_factor();
         const SpecRef ref{const_cast<cx<T> *>(in), ldh_, (size_t)(M_ + 1) * ldh_};
-        if (use_tma_)
-            k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, true><<<grid, RowNt<T>::value, row_smem(), stream_>>>(
-                plan_m_, post_, ref, map, H_, W_, B, FastDiv((uint32_t)B), scale, PlaneStore<T>{out, W_, nout_}, d_err_);
-        else
-            k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, false><<<grid, RowNt<T>::value, row_smem(), stream_>>>(
-                plan_m_, post_, ref, no_map_, H_, W_, B, FastDiv((uint32_t)B), scale, PlaneStore<T>{out, W_, nout_}, d_err_);
+        by_pad(plan_m_.pad_shift, [&](auto P) {
+            constexpr int PS = decltype(P)::value;
+            if (use_tma_)
+                k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, true, PS><<<grid, RowNt<T>::value, row_smem(), stream_>>>(
+                    plan_m_, post_, ref, map, H_, W_, B, FastDiv((uint32_t)B), scale, PlaneStore<T>{out, W_, nout_}, d_err_);
+            else
+                k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, false, PS><<<grid, RowNt<T>::value, row_smem(), stream_>>>(
+                    plan_m_, post_, ref, no_map_, H_, W_, B, FastDiv((uint32_t)B), scale, PlaneStore<T>{out, W_, nout_}, d_err_);
+        });
         UPDC_CUDA(cudaGetLastError());
     }
     T scale_factor() const {

@@ -392,10 +392,17 @@ template <int R, int NT, int CAP> struct StageK {
 // RMAX.  Stages run in descending radix order (fft_factor), one loop per
 // radix, so that only one radix's registers are live at a time (a single
 // switch inside one loop makes ptxas spill).
-template <bool INV, int NT, int CAP, int RMAX, typename T>
+// The plan's padding shift, or PADSH when a kernel is compiled for one
+// (PADSH = 31: no padding, so every fpad() folds away).
+template <int PADSH> __device__ __forceinline__ int plan_shift(const FftPlan &plan) {
+    if constexpr (PADSH >= 0) return PADSH;
+    else return plan.pad_shift;
+}
+
+template <bool INV, int NT, int CAP, int RMAX, int PADSH = -1, typename T>
 __device__ __forceinline__ void fft_batch(cx<T> *buf, int batch, const FftPlan &plan) {
     const cx<T> *tw = reinterpret_cast<const cx<T> *>(plan.tw);
-    const int n = plan.n, nstage = plan.nstage, sh = plan.pad_shift;
+    const int n = plan.n, nstage = plan.nstage, sh = plan_shift<PADSH>(plan);
     int s = 0;
 #define UPDC_FFT_RUN(R)                                                                                     \
     if constexpr (R <= RMAX) {                                                                             \

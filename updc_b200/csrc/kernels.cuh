@@ -199,12 +199,12 @@ __device__ __forceinline__ cx<T> c2r_input(cx<T> X, cx<T> Xm, int k, const cx<T>
 // blockIdx.y.
 // One block's tile: rows [y0, y0 + B) of plane `kexp`.  The block-level
 // body shared by the single-field kernel and the batched one (batch.cuh).
-template <typename T, int NT, int CAP, class Loader, bool TMA>
+template <typename T, int NT, int CAP, class Loader, bool TMA, int PADSH = -1>
 __device__ __forceinline__ void row_r2c_tile(const FftPlan &plan, const cx<T> *__restrict__ post, const Loader &ld,
                                              int W, int rows, int B, FastDiv bdiv, SpecRef out,
                                              const CUtensorMap *omap, int y0, int kexp, unsigned char *smem_raw) {
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
-    const int M = plan.n, sh = plan.pad_shift;
+    const int M = plan.n, sh = plan_shift<PADSH>(plan);
     const int nb = min(B, rows - y0);
     for (int b = 0; b < B; ++b)
         for (int m = threadIdx.x; m < M; m += NT) {
@@ -217,7 +217,7 @@ __device__ __forceinline__ void row_r2c_tile(const FftPlan &plan, const cx<T> *_
             buf[fpad(b * M + m, sh)] = {a, c};
         }
     __syncthreads();
-    fft_batch<false, NT, CAP, FFT_RMAX>(buf, B, plan);
+    fft_batch<false, NT, CAP, FFT_RMAX, PADSH>(buf, B, plan);
     if constexpr (TMA) {
         row_r2c_store_tma<T, NT, CAP>(buf, post, M, sh, B, nb, bdiv, omap, y0, kexp);
         return;
@@ -240,13 +240,13 @@ __device__ __forceinline__ void row_r2c_tile(const FftPlan &plan, const cx<T> *_
     }
 }
 
-template <typename T, int NT, int CAP, class Loader, bool TMA>
+template <typename T, int NT, int CAP, class Loader, bool TMA, int PADSH = -1>
 __global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
     k_row_r2c(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ post, Loader ld, int W, int rows, int B,
               FastDiv bdiv, SpecRef out, const __grid_constant__ CUtensorMap omap) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    row_r2c_tile<T, NT, CAP, Loader, TMA>(plan, post, ld, W, rows, B, bdiv, out, &omap, blockIdx.x * B, blockIdx.y,
-                                          smem_raw);
+    row_r2c_tile<T, NT, CAP, Loader, TMA, PADSH>(plan, post, ld, W, rows, B, bdiv, out, &omap, blockIdx.x * B,
+                                                 blockIdx.y, smem_raw);
 }
 
 // ---------------------------------------------------------------------------- row C2R
@@ -263,14 +263,14 @@ template <typename T> struct PlaneStore {
 // x in [0, W) of each row times `scale` (the crop of updc_core.c:765-766).
 // The imaginary parts of the DC and Nyquist bins are ignored, as FFTW does.
 // With TMA the block's {B rows} x {all u} tile arrives through the tensor map.
-template <typename T, int NT, int CAP, class Epi, bool TMA>
+template <typename T, int NT, int CAP, class Epi, bool TMA, int PADSH = -1>
 __device__ __forceinline__ void row_c2r_tile(const FftPlan &plan, const cx<T> *__restrict__ post, SpecRef in,
                                              const CUtensorMap *imap, int rows, int W, int B, FastDiv bdiv, T scale,
                                              const Epi &epi, unsigned long long *__restrict__ err, int y0, int kexp,
                                              unsigned char *smem_raw) {
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
     __shared__ __align__(8) uint64_t bar;
-    const int M = plan.n, sh = plan.pad_shift;
+    const int M = plan.n, sh = plan_shift<PADSH>(plan);
     const int nb = min(B, rows - y0);
     cx<T> *stage = buf;  // TMA: the tile arrives in the FFT buffer's memory
     const cx<T> *src = reinterpret_cast<const cx<T> *>(in.p) + kexp * in.batch_stride;
@@ -326,7 +326,7 @@ __device__ __forceinline__ void row_c2r_tile(const FftPlan &plan, const cx<T> *_
         }
     }
     __syncthreads();
-    fft_batch<true, NT, CAP, FFT_RMAX>(buf, B, plan);
+    fft_batch<true, NT, CAP, FFT_RMAX, PADSH>(buf, B, plan);
     for (int b = 0; b < nb; ++b)
         for (int x = threadIdx.x; x < W; x += NT) {
             const cx<T> z = buf[fpad(b * M + (x >> 1), sh)];
@@ -334,14 +334,14 @@ __device__ __forceinline__ void row_c2r_tile(const FftPlan &plan, const cx<T> *_
         }
 }
 
-template <typename T, int NT, int CAP, class Epi, bool TMA>
+template <typename T, int NT, int CAP, class Epi, bool TMA, int PADSH = -1>
 __global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
     k_row_c2r(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ post, SpecRef in,
               const __grid_constant__ CUtensorMap imap, int rows, int W, int B, FastDiv bdiv, T scale, Epi epi,
               unsigned long long *__restrict__ err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    row_c2r_tile<T, NT, CAP, Epi, TMA>(plan, post, in, &imap, rows, W, B, bdiv, scale, epi, err, blockIdx.x * B,
-                                       blockIdx.y, smem_raw);
+    row_c2r_tile<T, NT, CAP, Epi, TMA, PADSH>(plan, post, in, &imap, rows, W, B, bdiv, scale, epi, err,
+                                              blockIdx.x * B, blockIdx.y, smem_raw);
 }
 
 
@@ -365,13 +365,13 @@ __device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes) {
 // AUX = 1: the caller guarantees `aux` (global scratch) is given, so its
 // accesses compile to global loads and stores; AUX = 0 decides at run time
 // between `aux` and shared memory (generic accesses).
-template <typename T, int NT, int CAP, int AUX = 0>
+template <typename T, int NT, int CAP, int AUX = 0, int PADSH = -1>
 __device__ __forceinline__ void col_forward_column(const FftPlan &plan, const cx<T> *__restrict__ rx, int ldr,
                                                    int rows_in, const cx<T> *__restrict__ khat, size_t khat_stride,
                                                    int nexp, cx<T> *__restrict__ y, int ldy, size_t y_stride,
                                                    int rows_out, cx<T> *aux, int u, unsigned char *smem_raw) {
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
-    const int n = plan.n, sh = plan.pad_shift;
+    const int n = plan.n, sh = plan_shift<PADSH>(plan);
     cx<T> *xh;
     if constexpr (AUX == 1) xh = aux + (size_t)u * n;
     else xh = aux ? aux + (size_t)u * n : reinterpret_cast<cx<T> *>(smem_raw + fft_buf_bytes(n, sizeof(cx<T>), sh));
@@ -390,7 +390,7 @@ __device__ __forceinline__ void col_forward_column(const FftPlan &plan, const cx
             }
         }
         __syncthreads();
-        fft_batch<false, NT, CAP, FFT_RMAX>(buf, 1, plan);
+        fft_batch<false, NT, CAP, FFT_RMAX, PADSH>(buf, 1, plan);
         if (it == 0) {
             for (int v = threadIdx.x; v < n; v += NT) xh[v] = buf[fpad(v, sh)];
         } else {
@@ -404,14 +404,14 @@ __device__ __forceinline__ void col_forward_column(const FftPlan &plan, const cx
     }
 }
 
-template <typename T, int NT, int CAP, int AUX = 0>
+template <typename T, int NT, int CAP, int AUX = 0, int PADSH = -1>
 __global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_forward(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ rx, int ldr, int rows_in,
                                                     const cx<T> *__restrict__ khat, size_t khat_stride, int nexp,
                                                     cx<T> *__restrict__ y, int ldy, size_t y_stride, int rows_out,
                                                     int nu, cx<T> *aux) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     (void)nu;
-    col_forward_column<T, NT, CAP, AUX>(plan, rx, ldr, rows_in, khat, khat_stride, nexp, y, ldy, y_stride, rows_out,
+    col_forward_column<T, NT, CAP, AUX, PADSH>(plan, rx, ldr, rows_in, khat, khat_stride, nexp, y, ldy, y_stride, rows_out,
                                         aux, blockIdx.x, smem_raw);
 }
 
@@ -460,13 +460,13 @@ struct AccKahan {  // FP32 products, Kahan-compensated FP32 sum
 // for y < rows_out.  The sum over k runs in exposure order inside the block;
 // the final inverse goes through the same forward-FFT call site as
 // conj(FFT(conj(.))).
-template <typename T, class Acc, int NT, int CAP, int AUX = 0>
+template <typename T, class Acc, int NT, int CAP, int AUX = 0, int PADSH = -1>
 __device__ __forceinline__ void col_adjoint_column(const FftPlan &plan, const cx<T> *__restrict__ rs, int ldr,
                                                    size_t rs_stride, int rows_in, const cx<T> *__restrict__ khat,
                                                    size_t khat_stride, int nexp, cx<T> *__restrict__ c, int ldc,
                                                    int rows_out, typename Acc::S *aux, int u, unsigned char *smem_raw) {
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
-    const int n = plan.n, sh = plan.pad_shift;
+    const int n = plan.n, sh = plan_shift<PADSH>(plan);
     typename Acc::S *acc;
     if constexpr (AUX == 1) acc = aux + (size_t)u * n;
     else acc = aux ? aux + (size_t)u * n
@@ -484,7 +484,7 @@ __device__ __forceinline__ void col_adjoint_column(const FftPlan &plan, const cx
             }
         }
         __syncthreads();
-        fft_batch<false, NT, CAP, FFT_RMAX>(buf, 1, plan);
+        fft_batch<false, NT, CAP, FFT_RMAX, PADSH>(buf, 1, plan);
         if (it < nexp) {
             const cx<T> *kr = khat + it * khat_stride + (size_t)u * n;
             for (int v = threadIdx.x; v < n; v += NT) Acc::add(acc[v], buf[fpad(v, sh)], kr[v]);
@@ -499,27 +499,27 @@ __device__ __forceinline__ void col_adjoint_column(const FftPlan &plan, const cx
     }
 }
 
-template <typename T, class Acc, int NT, int CAP, int AUX = 0>
+template <typename T, class Acc, int NT, int CAP, int AUX = 0, int PADSH = -1>
 __global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_adjoint(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ rs, int ldr, size_t rs_stride,
                                                     int rows_in, const cx<T> *__restrict__ khat, size_t khat_stride, int nexp,
                                                     cx<T> *__restrict__ c, int ldc, int rows_out, typename Acc::S *aux) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    col_adjoint_column<T, Acc, NT, CAP, AUX>(plan, rs, ldr, rs_stride, rows_in, khat, khat_stride, nexp, c, ldc,
+    col_adjoint_column<T, Acc, NT, CAP, AUX, PADSH>(plan, rs, ldr, rs_stride, rows_in, khat, khat_stride, nexp, c, ldc,
                                              rows_out, aux, blockIdx.x, smem_raw);
 }
 
 // Plain column transform (setup: PSF spectra and generic 2-D transforms).
-template <typename T, int NT, int CAP, bool INV>
+template <typename T, int NT, int CAP, bool INV, int PADSH = -1>
 __global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_fft(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ in, int ldi, int rows_in,
                                                 cx<T> *__restrict__ out, int ldo, int rows_out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
-    const int n = plan.n, sh = plan.pad_shift;
+    const int n = plan.n, sh = plan_shift<PADSH>(plan);
     const int u = blockIdx.x;
     const cx<T> *src = in + (size_t)u * ldi;
     for (int v = threadIdx.x; v < n; v += NT) buf[fpad(v, sh)] = v < rows_in ? src[v] : cx<T>{0, 0};
     __syncthreads();
-    fft_batch<INV, NT, CAP, FFT_RMAX>(buf, 1, plan);
+    fft_batch<INV, NT, CAP, FFT_RMAX, PADSH>(buf, 1, plan);
     cx<T> *dst = out + (size_t)u * ldo;
     for (int v = threadIdx.x; v < rows_out; v += NT) dst[v] = buf[fpad(v, sh)];
 }
