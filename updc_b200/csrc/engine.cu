@@ -247,6 +247,11 @@ template <class F> void by_pad(int sh, F &&f) {
     if (sh == 31) f(std::integral_constant<int, 31>{});
     else f(std::integral_constant<int, -1>{});
 }
+// Same for the rows of a row tile (2, the usual FP32 tile, or read at run time).
+template <class F> void by_rows(int b, F &&f) {
+    if (b == 2) f(std::integral_constant<int, 2>{});
+    else f(std::integral_constant<int, 0>{});
+}
 template <typename T> using Caps = SpecCaps<T>;
 constexpr size_t SMEM_LIMIT = SPEC_SMEM_LIMIT;
 
@@ -987,12 +992,14 @@ template <typename T> class EngineImpl final : public Engine {
             dim3 grid((unsigned)ceil_div(H_, B), 1);
             float ms = 0;
             by_pad(plan.pad_shift, [&](auto P) {
-                constexpr int PS = decltype(P)::value;
-                set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false, PS>, smem);
-                ms = time_launch([&] {
-                    k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false, PS>
-                        <<<grid, RowNt<T>::value, smem, stream_>>>(plan, dpost, ld, W_, H_, B, FastDiv((uint32_t)B),
-                                                                   SpecRef{spec, H_, 0}, no_map_);
+                by_rows(B, [&](auto Q) {
+                    constexpr int PS = decltype(P)::value, BR = decltype(Q)::value;
+                    set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false, PS, BR>, smem);
+                    ms = time_launch([&] {
+                        k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false, PS, BR>
+                            <<<grid, RowNt<T>::value, smem, stream_>>>(plan, dpost, ld, W_, H_, B, FastDiv((uint32_t)B),
+                                                                       SpecRef{spec, H_, 0}, no_map_);
+                    });
                 });
             });
             ++*timed;
@@ -1255,11 +1262,13 @@ template <typename T> class EngineImpl final : public Engine {
     void configure_kernels() {
         const size_t rs = row_smem();
         by_pad(plan_m_.pad_shift, [&](auto P) {
-            constexpr int PS = decltype(P)::value;
-            set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, true, PS>, rs);
-            set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false, PS>, rs);
-            set_smem(k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, true, PS>, rs);
-            set_smem(k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, false, PS>, rs);
+            by_rows(row_b_, [&](auto Q) {
+                constexpr int PS = decltype(P)::value, BR = decltype(Q)::value;
+                set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, true, PS, BR>, rs);
+                set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false, PS, BR>, rs);
+                set_smem(k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, true, PS, BR>, rs);
+                set_smem(k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, false, PS, BR>, rs);
+            });
         });
         const size_t fs = fwd_smem();
         by_pad(plan_h_.pad_shift, [&](auto P) {
@@ -1296,13 +1305,15 @@ template <typename T> class EngineImpl final : public Engine {
         const PlaneLoader<T> ld{plane, W_, plane_stride};
         const SpecRef ref{out, ldh_, (size_t)(M_ + 1) * ldh_};
         by_pad(plan_m_.pad_shift, [&](auto P) {
-            constexpr int PS = decltype(P)::value;
-            if (use_tma_)
-                k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, true, PS><<<grid, RowNt<T>::value, row_smem(), stream_>>>(
-                    plan_m_, post_, ld, W_, H_, B, FastDiv((uint32_t)B), ref, map);
-            else
-                k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false, PS><<<grid, RowNt<T>::value, row_smem(), stream_>>>(
-                    plan_m_, post_, ld, W_, H_, B, FastDiv((uint32_t)B), ref, no_map_);
+            by_rows(B, [&](auto Q) {
+                constexpr int PS = decltype(P)::value, BR = decltype(Q)::value;
+                if (use_tma_)
+                    k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, true, PS, BR><<<grid, RowNt<T>::value, row_smem(), stream_>>>(
+                        plan_m_, post_, ld, W_, H_, B, FastDiv((uint32_t)B), ref, map);
+                else
+                    k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false, PS, BR><<<grid, RowNt<T>::value, row_smem(), stream_>>>(
+                        plan_m_, post_, ld, W_, H_, B, FastDiv((uint32_t)B), ref, no_map_);
+            });
         });
         UPDC_CUDA(cudaGetLastError());
     }
@@ -1351,13 +1362,15 @@ template <typename T> class EngineImpl final : public Engine {
         const T scale = scale_factor();
         const SpecRef ref{const_cast<cx<T> *>(in), ldh_, (size_t)(M_ + 1) * ldh_};
         by_pad(plan_m_.pad_shift, [&](auto P) {
-            constexpr int PS = decltype(P)::value;
-            if (use_tma_)
-                k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, true, PS><<<grid, RowNt<T>::value, row_smem(), stream_>>>(
-                    plan_m_, post_, ref, map, H_, W_, B, FastDiv((uint32_t)B), scale, PlaneStore<T>{out, W_, nout_}, d_err_);
-            else
-                k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, false, PS><<<grid, RowNt<T>::value, row_smem(), stream_>>>(
-                    plan_m_, post_, ref, no_map_, H_, W_, B, FastDiv((uint32_t)B), scale, PlaneStore<T>{out, W_, nout_}, d_err_);
+            by_rows(B, [&](auto Q) {
+                constexpr int PS = decltype(P)::value, BR = decltype(Q)::value;
+                if (use_tma_)
+                    k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, true, PS, BR><<<grid, RowNt<T>::value, row_smem(), stream_>>>(
+                        plan_m_, post_, ref, map, H_, W_, B, FastDiv((uint32_t)B), scale, PlaneStore<T>{out, W_, nout_}, d_err_);
+                else
+                    k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, false, PS, BR><<<grid, RowNt<T>::value, row_smem(), stream_>>>(
+                        plan_m_, post_, ref, no_map_, H_, W_, B, FastDiv((uint32_t)B), scale, PlaneStore<T>{out, W_, nout_}, d_err_);
+            });
         });
         UPDC_CUDA(cudaGetLastError());
     }

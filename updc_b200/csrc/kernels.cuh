@@ -109,6 +109,13 @@ __host__ __device__ inline size_t row_stage_bytes(int B, int M, size_t csize) {
     return (size_t)row_nbox(M) * row_ubox(M) * B * csize;
 }
 
+// Division by the rows of a row tile: by a compile-time B where the kernel is
+// compiled for one (BR > 0), else with the runtime divisor.
+template <int BR> __device__ __forceinline__ int div_rows(const FastDiv &d, int q) {
+    if constexpr (BR > 0) return q / BR;
+    else return (int)d.div((uint32_t)q);
+}
+
 // ---------------------------------------------------------------------------- TMA tiles in place
 // With TMA the row kernels stage the block's u-major tile ({all bins} x {B
 // rows}, box by box) in the same shared memory as the FFT buffer: every
@@ -138,9 +145,10 @@ __device__ __forceinline__ cx<T> r2c_bin(const cx<T> *buf, int row0, int u, int 
     return {E.x + P.y, E.y - P.x};
 }
 
-template <typename T, int NT, int CAP>
+template <typename T, int NT, int CAP, int BR = 0>
 __device__ __forceinline__ void row_r2c_store_tma(cx<T> *buf, const cx<T> *__restrict__ post, int M, int sh, int B,
                                                   int nb, FastDiv bdiv, const CUtensorMap *omap, int y0, int kexp) {
+    if constexpr (BR > 0) B = BR;
     constexpr int KP = RowPairs<CAP, NT>::value;
     const int npairs = (M / 2 + 1) * B;
     cx<T> xa[KP], xb[KP];
@@ -149,7 +157,7 @@ __device__ __forceinline__ void row_r2c_store_tma(cx<T> *buf, const cx<T> *__res
         const int q = threadIdx.x + j * NT;
         xa[j] = xb[j] = cx<T>{T(0), T(0)};
         if (q < npairs) {
-            const int u = (int)bdiv.div((uint32_t)q), b = q - u * B;
+            const int u = div_rows<BR>(bdiv, q), b = q - u * B;
             if (b < nb) {
                 xa[j] = r2c_bin(buf, b * M, u, M, sh, post);
                 xb[j] = r2c_bin(buf, b * M, M - u, M, sh, post);
@@ -162,7 +170,7 @@ __device__ __forceinline__ void row_r2c_store_tma(cx<T> *buf, const cx<T> *__res
     for (int j = 0; j < KP; ++j) {
         const int q = threadIdx.x + j * NT;
         if (q < npairs) {
-            const int u = (int)bdiv.div((uint32_t)q), b = q - u * B;
+            const int u = div_rows<BR>(bdiv, q), b = q - u * B;
             stage[u * B + b] = xa[j];
             if (M - u != u) stage[(M - u) * B + b] = xb[j];
         }
@@ -199,10 +207,11 @@ __device__ __forceinline__ cx<T> c2r_input(cx<T> X, cx<T> Xm, int k, const cx<T>
 // blockIdx.y.
 // One block's tile: rows [y0, y0 + B) of plane `kexp`.  The block-level
 // body shared by the single-field kernel and the batched one (batch.cuh).
-template <typename T, int NT, int CAP, class Loader, bool TMA, int PADSH = -1>
+template <typename T, int NT, int CAP, class Loader, bool TMA, int PADSH = -1, int BR = 0>
 __device__ __forceinline__ void row_r2c_tile(const FftPlan &plan, const cx<T> *__restrict__ post, const Loader &ld,
                                              int W, int rows, int B, FastDiv bdiv, SpecRef out,
                                              const CUtensorMap *omap, int y0, int kexp, unsigned char *smem_raw) {
+    if constexpr (BR > 0) B = BR;
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
     const int M = plan.n, sh = plan_shift<PADSH>(plan);
     const int nb = min(B, rows - y0);
@@ -219,13 +228,13 @@ __device__ __forceinline__ void row_r2c_tile(const FftPlan &plan, const cx<T> *_
     __syncthreads();
     fft_batch<false, NT, CAP, FFT_RMAX, PADSH>(buf, B, plan);
     if constexpr (TMA) {
-        row_r2c_store_tma<T, NT, CAP>(buf, post, M, sh, B, nb, bdiv, omap, y0, kexp);
+        row_r2c_store_tma<T, NT, CAP, BR>(buf, post, M, sh, B, nb, bdiv, omap, y0, kexp);
         return;
     }
     cx<T> *dst = reinterpret_cast<cx<T> *>(out.p) + kexp * out.batch_stride;
     const T half = T(0.5);
     for (int i = threadIdx.x; i < (M + 1) * B; i += NT) {
-        const int u = (int)bdiv.div((uint32_t)i), b = i - u * B;
+        const int u = div_rows<BR>(bdiv, i), b = i - u * B;
         cx<T> X = {0, 0};
         if (b < nb) {
             const cx<T> Z = buf[fpad(b * M + (u == M ? 0 : u), sh)];
@@ -240,13 +249,13 @@ __device__ __forceinline__ void row_r2c_tile(const FftPlan &plan, const cx<T> *_
     }
 }
 
-template <typename T, int NT, int CAP, class Loader, bool TMA, int PADSH = -1>
+template <typename T, int NT, int CAP, class Loader, bool TMA, int PADSH = -1, int BR = 0>
 __global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
     k_row_r2c(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ post, Loader ld, int W, int rows, int B,
               FastDiv bdiv, SpecRef out, const __grid_constant__ CUtensorMap omap) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    row_r2c_tile<T, NT, CAP, Loader, TMA, PADSH>(plan, post, ld, W, rows, B, bdiv, out, &omap, blockIdx.x * B,
-                                                 blockIdx.y, smem_raw);
+    row_r2c_tile<T, NT, CAP, Loader, TMA, PADSH, BR>(plan, post, ld, W, rows, BR > 0 ? BR : B, bdiv, out, &omap,
+                                                     blockIdx.x * (BR > 0 ? BR : B), blockIdx.y, smem_raw);
 }
 
 // ---------------------------------------------------------------------------- row C2R
@@ -263,11 +272,12 @@ template <typename T> struct PlaneStore {
 // x in [0, W) of each row times `scale` (the crop of updc_core.c:765-766).
 // The imaginary parts of the DC and Nyquist bins are ignored, as FFTW does.
 // With TMA the block's {B rows} x {all u} tile arrives through the tensor map.
-template <typename T, int NT, int CAP, class Epi, bool TMA, int PADSH = -1>
+template <typename T, int NT, int CAP, class Epi, bool TMA, int PADSH = -1, int BR = 0>
 __device__ __forceinline__ void row_c2r_tile(const FftPlan &plan, const cx<T> *__restrict__ post, SpecRef in,
                                              const CUtensorMap *imap, int rows, int W, int B, FastDiv bdiv, T scale,
                                              const Epi &epi, unsigned long long *__restrict__ err, int y0, int kexp,
                                              unsigned char *smem_raw) {
+    if constexpr (BR > 0) B = BR;
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
     __shared__ __align__(8) uint64_t bar;
     const int M = plan.n, sh = plan_shift<PADSH>(plan);
@@ -299,7 +309,7 @@ __device__ __forceinline__ void row_c2r_tile(const FftPlan &plan, const cx<T> *_
             const int q = threadIdx.x + j * NT;
             za[j] = zb[j] = cx<T>{T(0), T(0)};
             if (q < npairs) {
-                const int k = (int)bdiv.div((uint32_t)q), b = q - k * B;
+                const int k = div_rows<BR>(bdiv, q), b = q - k * B;
                 if (b < nb) {
                     const cx<T> X = stage[k * B + b], Xm = stage[(M - k) * B + b];
                     za[j] = c2r_input(X, Xm, k, post);
@@ -312,14 +322,14 @@ __device__ __forceinline__ void row_c2r_tile(const FftPlan &plan, const cx<T> *_
         for (int j = 0; j < KP; ++j) {
             const int q = threadIdx.x + j * NT;
             if (q < npairs) {
-                const int k = (int)bdiv.div((uint32_t)q), b = q - k * B;
+                const int k = div_rows<BR>(bdiv, q), b = q - k * B;
                 buf[fpad(b * M + k, sh)] = za[j];
                 if (k > 0 && M - k != k) buf[fpad(b * M + M - k, sh)] = zb[j];
             }
         }
     } else {
         for (int i = threadIdx.x; i < M * B; i += NT) {
-            const int k = (int)bdiv.div((uint32_t)i), b = i - k * B;
+            const int k = div_rows<BR>(bdiv, i), b = i - k * B;
             cx<T> Zp = {0, 0};
             if (b < nb) Zp = c2r_input(src[(size_t)k * in.ld + y0 + b], src[(size_t)(M - k) * in.ld + y0 + b], k, post);
             buf[fpad(b * M + k, sh)] = Zp;
@@ -334,14 +344,14 @@ __device__ __forceinline__ void row_c2r_tile(const FftPlan &plan, const cx<T> *_
         }
 }
 
-template <typename T, int NT, int CAP, class Epi, bool TMA, int PADSH = -1>
+template <typename T, int NT, int CAP, class Epi, bool TMA, int PADSH = -1, int BR = 0>
 __global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
     k_row_c2r(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ post, SpecRef in,
               const __grid_constant__ CUtensorMap imap, int rows, int W, int B, FastDiv bdiv, T scale, Epi epi,
               unsigned long long *__restrict__ err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    row_c2r_tile<T, NT, CAP, Epi, TMA, PADSH>(plan, post, in, &imap, rows, W, B, bdiv, scale, epi, err,
-                                              blockIdx.x * B, blockIdx.y, smem_raw);
+    row_c2r_tile<T, NT, CAP, Epi, TMA, PADSH, BR>(plan, post, in, &imap, rows, W, BR > 0 ? BR : B, bdiv, scale, epi,
+                                                  err, blockIdx.x * (BR > 0 ? BR : B), blockIdx.y, smem_raw);
 }
 
 
