@@ -587,7 +587,10 @@ def b200_arm(args, rank, world, local_rank):
     w = synth.WORKLOADS[args.workload]
     workdir = Path(args.data_dir or tempfile.mkdtemp(prefix=f"updc_bench_r{rank}_"))
     ds = synth.generate(w.name, workdir, use_torch=True)
-    eng = Engine(form=args.form, device=local_rank, autotune=not args.no_autotune, tune_cache_dir=workdir)
+    tune_dir = args.tune_cache or workdir
+    if args.tune_cache:
+        Path(tune_dir).mkdir(parents=True, exist_ok=True)
+    eng = Engine(form=args.form, device=local_rank, autotune=not args.no_autotune, tune_cache_dir=str(tune_dir))
     eng.load(str(ds.manifest), w.W, w.H, w.iw, w.ih, w.nexp)
     t0 = time.time()
     eng.setup()
@@ -704,6 +707,8 @@ def main():
     p.add_argument("--replicas", action="store_true",
                    help="with N > 1: N independent replicas instead of exposure shards of one field")
     p.add_argument("--fields", type=int, default=64, help="fields of the batched workload (c2)")
+    p.add_argument("--tune-cache", default=None,
+                   help="directory of the FFT autotuner's cache (a profiled rerun then uses the same plans)")
     p.add_argument("--no-autotune", action="store_true",
                    help="smallest 7-smooth FFT shape and greedy radix splits instead of the device autotuner")
     p.add_argument("--no-fp64-check", action="store_true",
