@@ -159,8 +159,8 @@ def model_bytes(w, fw, fh, links, dtype_bytes=4):
 # FFT 3584^2): the kernels' traffic grows in proportion to the columns, rows
 # and exposures they process, so this ratio carries a capture of the small
 # case to the benchmark's workload.
-TRAFFIC_RATIO_C3 = {"estimate_x_pass": 18.0 / 46.2, "forward_y_passes": 368.8 / 352.5, "forward_x_pass": 158.1 / 184.6,
-                    "scatter_x_pass": 131.0 / 184.6, "adjoint_y_x_passes": (431.2 + 29.0) / (352.5 + 46.2)}
+TRAFFIC_RATIO_C3 = {"estimate_x_pass": 21.0 / 46.2, "forward_y_passes": 385.3 / 352.5, "forward_x_pass": 158.9 / 184.6,
+                    "scatter_x_pass": 150.9 / 184.6, "adjoint_y_x_passes": (443.1 + 29.7) / (352.5 + 46.2)}
 
 STAGES = ["estimate_x_pass", "forward_y_passes", "forward_x_pass", "detector", "adjoint_gather",
           "scatter_x_pass", "adjoint_y_x_passes", "update"]
