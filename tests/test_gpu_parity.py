@@ -130,6 +130,28 @@ def test_large_column_transforms(engine_lib, oracle, datasets, form, tol):
     assert rel_rms(e2.plane("estimate", as_double=True), s64.estimate) <= 10 * tol
 
 
+@pytest.mark.parametrize("width", [3600, 3840])
+@pytest.mark.parametrize("form,tol", [("fp32", 2e-6), ("fp64", 1e-12)])
+def test_two_row_tiles(engine_lib, oracle, datasets, form, tol, width):
+    """FFT widths whose rows go two to a tile (the row kernels' two-row
+    instantiation, with TMA tiles): 3600 gets an unpadded row plan (the
+    no-padding instantiation), 3840 a padded one.  Forward model and two
+    iterations against the FP64 oracle on the same shape."""
+    ds = datasets("c0")
+    shape = (width, 288)
+    e = _engine(ds, form=form, fft_shape=shape)
+    assert e.fft_shape == shape
+    s64 = _oracle_solver(oracle, ds, precision=64, fft_shape=shape)
+    e.set_plane("estimate", s64.estimate)
+    e.stage_forward()
+    for k in range(ds.workload.nexp):
+        assert rel_rms(e.plane("blur", k, as_double=True), s64.forward_blur(k)) <= tol
+    e2 = _engine(ds, form=form, fft_shape=shape)
+    e2.iterate(2)
+    s64.iterate(2)
+    assert rel_rms(e2.plane("estimate", as_double=True), s64.estimate) <= 10 * tol
+
+
 # ---------------------------------------------------------------------------- detector / update
 @pytest.mark.parametrize("background", [None, -100.0])
 def test_detector_and_adjoint_gather_bit_exact(engine_lib, oracle, datasets, background):
