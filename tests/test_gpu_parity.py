@@ -130,15 +130,14 @@ def test_large_column_transforms(engine_lib, oracle, datasets, form, tol):
     assert rel_rms(e2.plane("estimate", as_double=True), s64.estimate) <= 10 * tol
 
 
-@pytest.mark.parametrize("width", [3600, 3840])
+@pytest.mark.parametrize("shape", [(3600, 300), (3840, 288)])
 @pytest.mark.parametrize("form,tol", [("fp32", 2e-6), ("fp64", 1e-12)])
-def test_two_row_tiles(engine_lib, oracle, datasets, form, tol, width):
+def test_two_row_tiles(engine_lib, oracle, datasets, form, tol, shape):
     """FFT widths whose rows go two to a tile (the row kernels' two-row
-    instantiation, with TMA tiles): 3600 gets an unpadded row plan (the
-    no-padding instantiation), 3840 a padded one.  Forward model and two
-    iterations against the FP64 oracle on the same shape."""
+    instantiation, with TMA tiles).  3600 x 300 gets unpadded row and column
+    plans (the no-padding instantiations), 3840 x 288 padded ones.  Forward
+    model and two iterations against the FP64 oracle on the same shape."""
     ds = datasets("c0")
-    shape = (width, 288)
     e = _engine(ds, form=form, fft_shape=shape)
     assert e.fft_shape == shape
     s64 = _oracle_solver(oracle, ds, precision=64, fft_shape=shape)
