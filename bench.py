@@ -278,6 +278,56 @@ def cpu_baseline_sample(ds, w):
                       f"(fft_workers={fftw}, exposure_workers={w.nexp}, FFTW-API shim FFT)"}
 
 
+def reference_check(ds, w, form, device, **engine_kw):
+    """The metric's accuracy side against the reference itself: a fresh engine
+    of the timed form and the reference core (oracle/_ref, on this machine's
+    host cores, warm caches) both run the workload's full iteration count on
+    the same files; reported are the relative RMS and the largest relative
+    error of the final x against the reference's, the per-iteration FreezeMu
+    count rows that differ from the reference's freeze CSV
+    (updc_core.c:1425-1431), the largest relative difference of min raw_mu,
+    and the reference's own per-iteration times (the CPU baseline)."""
+    import numpy as np
+    from oracle import oracle as O
+    from updc_b200.engine import Engine
+    if not O.REF_BINARY.is_file():
+        return None
+    cores = os.cpu_count() or 1
+    fftw = max(1, cores // w.nexp)
+    e = Engine(form=form, device=device, **engine_kw)
+    e.load(str(ds.manifest), w.W, w.H, w.iw, w.ih, w.nexp).setup()
+    st = e.iterate(w.iterations, check_each=False)
+    x = e.plane("estimate", as_double=True)
+    mine = [(int(s.new_frozen[k]), int(s.total_frozen[k]), float(s.min_raw_mu[k])) for s in st for k in range(w.nexp)]
+    e.close()
+    a = ds.engine_args(iterations=w.iterations, prefix="refcheck", fft_workers=fftw, exposure_workers=w.nexp,
+                       preprocess_workers=w.nexp).argv()
+    t0 = time.time()
+    r = subprocess.run([str(O.REF_BINARY), *a], capture_output=True, text=True,
+                       env={**os.environ, "UPDC_PERSIST_CACHE": "1"}, timeout=3600)
+    wall = time.time() - t0
+    if r.returncode:
+        return {"error": r.stderr[-300:]}
+    xr = np.fromfile(f"{ds.directory}/refcheck_{w.iterations:02d}.bin", np.float32).reshape(w.H, w.W).astype(np.float64)
+    d = x - xr
+    mask = np.abs(xr) > 1e-8 * np.abs(xr).max()
+    with open(f"{ds.directory}/refcheck_mufreeze.csv") as f:
+        rows = list(csv.DictReader(f))
+    count_mismatch = sum(1 for (a1, b1, _), q in zip(mine, rows)
+                         if (a1, b1) != (int(q["n_new_frozen"]), int(q["n_total_frozen"])))
+    mu_rel = max((abs(m - float(q["min_raw_mu"])) / max(abs(float(q["min_raw_mu"])), 1e-30)
+                  for (_, _, m), q in zip(mine, rows)), default=0.0)
+    trow = list(csv.reader(open(f"{ds.directory}/refcheck_timing.csv")))
+    its = [float(v) for k, v in trow[1:] if k.startswith("iteration_") and k.endswith("_total")]
+    return {"form": form, "iterations": w.iterations,
+            "rel_rms": float(np.sqrt(np.mean(d * d) / np.mean(xr * xr))),
+            "max_rel_masked": float(np.max(np.abs(d[mask]) / np.abs(xr[mask]))),
+            "freeze_rows": len(rows), "freeze_count_rows_differing": count_mismatch,
+            "frozen_total_reference": int(sum(int(q["n_new_frozen"]) for q in rows)),
+            "min_raw_mu_max_rel_diff": mu_rel, "reference_wall_s": round(wall, 1),
+            "reference_iteration_ms": [round(1000.0 * v, 1) for v in its], "cores": cores, "fft_workers": fftw}
+
+
 def fp64_comparison(eng, ds, w, args, device):
     """The metric's accuracy side: run the FP64 form (the GPU oracle) on the
     same inputs to the workload's full iteration count, bring the timed engine
@@ -643,8 +693,22 @@ def b200_arm(args, rank, world, local_rank):
     if args.form != "fp64" and not args.no_fp64_check:
         fp64 = fp64_comparison(eng, ds, w, args, local_rank)
     cpu = None
+    refcheck = None
+    if rank == 0 and world == 1 and not args.no_reference_check:
+        refcheck = reference_check(ds, w, args.form, local_rank, autotune=not args.no_autotune,
+                                   tune_cache_dir=str(tune_dir))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(ds, w)
+        its = (refcheck or {}).get("reference_iteration_ms")
+        if its and len(its) > 1:
+            # the reference run of the accuracy check is the CPU baseline sample
+            timed = its[1:]
+            cpu = {"value": round(statistics.mean(timed), 1), "unit": "ms", "cores": refcheck["cores"],
+                   "kind": "reference",
+                   "sample": f"iterations 2-{len(its)} of the reference core's {len(its)}-iteration run on the same "
+                             f"{w.name} inputs (fft_workers={refcheck['fft_workers']}, exposure_workers={w.nexp}, "
+                             f"warm caches, FFTW-API shim FFT)"}
+        else:
+            cpu = cpu_baseline_sample(ds, w)
     # estimate R2C, column forward, forward C2R (all exposures), detector,
     # adjoint gather, scatter R2C (all exposures), column adjoint, adjoint
     # C2R, update, reduction
@@ -652,7 +716,9 @@ def b200_arm(args, rank, world, local_rank):
     result = {
         "metric": "ms/iteration", "value": round(ms, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32",
+        # one fixed field at every N: strong, unless N independent replicas run
+        "scaling": "weak" if world > 1 else "strong", "vs_baseline": None,
+        "dtype": "f64" if args.form == "fp64" else "f32",
         "data": "synthetic",
         "config": {"workload": args.workload, "form": args.form, "target": [w.W, w.H], "exposures": w.nexp,
                    "detector": [w.iw, w.ih], "psf": w.psf_size, "fft": [fw, fh],
@@ -679,6 +745,7 @@ def b200_arm(args, rank, world, local_rank):
                 "d2h_bytes_per_step": x.itemsize * nout},
         "cufft_reference": cufft,
         "fp64_check": fp64,
+        "reference_check": refcheck,
         "speedup_vs_fp64": round(fp64["fp64_ms_per_iteration"] / ms, 3) if fp64 else None,
         "gpu_launches": launches_per_iter * args.steps,
         "clocks": clocks.summary(),
@@ -713,6 +780,8 @@ def main():
                    help="smallest 7-smooth FFT shape and greedy radix splits instead of the device autotuner")
     p.add_argument("--no-fp64-check", action="store_true",
                    help="skip the FP64-form run that gives the metric's accuracy side")
+    p.add_argument("--no-reference-check", action="store_true",
+                   help="skip the full-length run of the reference core that the final x is compared with")
     args = p.parse_args()
     rank, world, local_rank = env_rank()
     if args.impl == "reference":

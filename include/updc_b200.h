@@ -45,13 +45,18 @@ typedef struct {
     int device;          /* CUDA device ordinal */
     int reuse_links;     /* reuse a valid <vertices>.links file instead of rebuilding */
     int verbose;
-    int fft_width;       /* 0: smallest even 7-smooth >= W + pw - 1 */
-    int fft_height;      /* 0: smallest 7-smooth >= H + ph - 1 */
+    int fft_width;       /* 0: smallest even 7-smooth >= the minimum width (see fft_linear) */
+    int fft_height;      /* 0: smallest 7-smooth >= the minimum height (see fft_linear) */
     int stage_timing;    /* per-stage CUDA-event timing (disables the graph) */
     int autotune;        /* time candidate FFT shapes and radix splits on the device at setup
                             (select_fft_shape, updc_core.c:242-291) */
     int retune;          /* ignore a cached autotune choice */
     const char *tune_cache_dir; /* directory of the autotune cache; NULL or "" = none */
+    int fft_linear;      /* minimum FFT lengths: 1 = W + pw - 1, H + ph - 1, the full linear
+                            convolution (updc_core.c:1335-1341); 0 (default) = W + pw/2, H + ph/2:
+                            only the W x H window of each circular convolution is kept, and with
+                            the PSF centred at offset -pw/2 (updc_core.c:814-819) that window is
+                            already exactly the linear convolution's at this length */
 } updc_options;
 
 typedef struct {
@@ -120,8 +125,9 @@ int updc_stage_update(updc_engine *h, double *signed_sum, uint64_t *negative);
  *     its scratch is one file-scope __device__ array of
  *     UPDC_UPDATE_NOALLOC_SCRATCH_BYTES bytes per device;
  *   - the first call on each device looks the scratch up with
- *     cudaGetSymbolAddress; make that first call before any stream capture
- *     begins on the device;
+ *     cudaGetSymbolAddress, and so does the first call after the device's
+ *     context changed (cudaDeviceReset); make those calls before any stream
+ *     capture begins on the device;
  *   - nothing in the scratch has to start at zero: each call first sets the
  *     error record to "none", and every partial slot is written before it is
  *     read;

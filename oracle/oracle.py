@@ -20,7 +20,8 @@ LIB_PATH = HERE / "_build" / "liboracle.so"
 SHIM_PATH = HERE / "_build" / "libfftw_shim.so"
 REF_BINARY = HERE / "_ref" / "updc_jwst_c"
 REF_PROJECTOR = HERE / "_ref" / "updc_psf_projector"
-REFERENCE_SOURCES = Path("/root/reference/updc/c_core")
+# the reference checkout: UPDC_REFERENCE_DIR, by default a sibling of this repository
+REFERENCE_SOURCES = Path(os.environ.get("UPDC_REFERENCE_DIR", HERE.parent.parent / "reference")) / "updc" / "c_core"
 
 _lib = None
 

@@ -89,6 +89,18 @@ def fft_shape_for(ds, even_width: bool = True):
     return fw, O.next_fast_size(w.H + ph - 1)
 
 
+def crop_min_shape(ds, transposed: bool = False):
+    """Smallest circular lengths whose kept W x H window is exactly the linear
+    convolution's: n + f/2 per axis (and at least f), with f the largest PSF
+    extent along that axis."""
+    w = ds.workload
+    pw = max(r.psf_width for r in ds.rows)
+    ph = max(r.psf_height for r in ds.rows)
+    if transposed:
+        pw, ph = ph, pw
+    return max(w.W + pw // 2, pw), max(w.H + ph // 2, ph)
+
+
 def rel_rms(a, b):
     import numpy as np
     a = np.asarray(a, np.float64)

@@ -22,6 +22,7 @@ import hashlib
 import io
 import json
 import sys
+import os
 import tempfile
 import types
 from pathlib import Path
@@ -30,7 +31,8 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
-REFERENCE = Path("/root/reference")
+# the reference checkout: UPDC_REFERENCE_DIR, by default a sibling of this repository
+REFERENCE = Path(os.environ.get("UPDC_REFERENCE_DIR", ROOT.parent / "reference"))
 OUT = HERE / "preprocess"
 sys.path.insert(0, str(ROOT))
 

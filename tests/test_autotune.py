@@ -5,7 +5,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from conftest import fft_shape_for
+from conftest import crop_min_shape
 
 
 @pytest.mark.gpu
@@ -13,7 +13,7 @@ def test_autotune_choice_cache_and_results(engine_lib, datasets, tmp_path):
     from updc_b200.engine import Engine
     ds = datasets("medium")
     w = ds.workload
-    min_w, min_h = fft_shape_for(ds, even_width=False)   # smallest 7-smooth sizes (reference rule)
+    min_w, min_h = crop_min_shape(ds)   # shapes below these would change the kept window
 
     def run(**kw):
         e = Engine(form="fp32", **kw)

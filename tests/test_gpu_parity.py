@@ -111,6 +111,34 @@ def test_forward_model_vs_fp64_oracle(engine_lib, oracle, datasets, form, tol):
 
 
 @pytest.mark.parametrize("form,tol", [("fp32", 2e-6), ("fp64", 1e-12)])
+def test_minimum_fft_shape_rules(engine_lib, oracle, datasets, form, tol):
+    """The default shape is the smallest 7-smooth one >= W + pw/2 (even width),
+    the fft_linear one the reference's smallest >= W + pw - 1; the forward
+    model on the smaller shape equals the FP64 oracle's on the reference's
+    shape, and so does the denominator (the kept window is exact)."""
+    from conftest import crop_min_shape
+    ds = datasets("medium")
+    w = ds.workload
+    s64 = _oracle_solver(oracle, ds, precision=64)
+    lin = _engine(ds, form=form, fft_linear=True)
+    assert lin.fft_shape == fft_shape_for(ds)
+    crop = _engine(ds, form=form)
+    cw, ch = crop_min_shape(ds)
+    fw, fh = crop.fft_shape
+    assert fw % 2 == 0 and fw >= cw and fh >= ch
+    assert fw < lin.fft_shape[0] and fh < lin.fft_shape[1]
+    assert all(oracle.next_fast_size(v) == v for v in (fw, fh))
+    assert rel_rms(crop.plane("denominator", as_double=True), s64.denominator) <= tol
+    for e in (crop, lin):
+        e.set_plane("estimate", s64.estimate)
+        e.stage_forward()
+        for k in range(w.nexp):
+            assert rel_rms(e.plane("blur", k, as_double=True), s64.forward_blur(k)) <= tol
+    crop.close()
+    lin.close()
+
+
+@pytest.mark.parametrize("form,tol", [("fp32", 2e-6), ("fp64", 1e-12)])
 def test_large_column_transforms(engine_lib, oracle, datasets, form, tol):
     """FFT heights above the small column capacity (the 11264-point kernels;
     FP64 keeps X-hat and the adjoint accumulator in global memory): forward

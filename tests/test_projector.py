@@ -76,3 +76,26 @@ def test_gpu_projector_rejects_like_the_reference(engine_lib, reference_projecto
                           capture_output=True, text=True)
     assert ref.returncode == ours.returncode == 1
     assert ours.stderr.strip() == ref.stderr.strip() == "UPDC_PSF_PROJECT: PSF contains negative/non-finite pixels"
+
+
+@pytest.mark.parametrize("text", [
+    "",                                             # empty
+    "# only a comment\n\n",                         # comments and blank lines only
+    "a.f32\t33\t33\tv.bin\n",                       # too few fields
+    "a.f32\t0\t33\tv.bin\to.f32\tlabel\n",          # invalid dimensions
+    "a.f32\t33\t-2\tv.bin\to.f32\tlabel\n",
+    "x" * 1100 + "\t33\t33\tv.bin\to.f32\tlabel\n",  # path too long
+    "\r\n",                                         # a CR-only line is a row without fields
+])
+def test_projector_manifest_errors_like_the_reference(engine_lib, reference_projector, tmp_path, text):
+    """Manifest rows the projectors reject before any projection (no GPU work):
+    the same message and exit status as the reference projector."""
+    from updc_b200 import _lib
+    exe = _lib.LIB_PATH.parent / "bin" / "updc_psf_projector"
+    m = tmp_path / "m.txt"
+    m.write_text(text)
+    ref = subprocess.run([str(reference_projector), str(m), "1", str(tmp_path / "r.csv")],
+                         capture_output=True, text=True)
+    ours = subprocess.run([str(exe), str(m), "1", str(tmp_path / "g.csv")], capture_output=True, text=True)
+    assert ref.returncode == ours.returncode == 1
+    assert ours.stderr == ref.stderr

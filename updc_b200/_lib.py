@@ -27,7 +27,8 @@ class Options(ctypes.Structure):
     _fields_ = [("form", ctypes.c_int), ("compensated_mu", ctypes.c_int), ("use_graph", ctypes.c_int),
                 ("device", ctypes.c_int), ("reuse_links", ctypes.c_int), ("verbose", ctypes.c_int),
                 ("fft_width", ctypes.c_int), ("fft_height", ctypes.c_int), ("stage_timing", ctypes.c_int),
-                ("autotune", ctypes.c_int), ("retune", ctypes.c_int), ("tune_cache_dir", ctypes.c_char_p)]
+                ("autotune", ctypes.c_int), ("retune", ctypes.c_int), ("tune_cache_dir", ctypes.c_char_p),
+                ("fft_linear", ctypes.c_int)]
 
 
 class IterStats(ctypes.Structure):

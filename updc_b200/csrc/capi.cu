@@ -66,6 +66,7 @@ EngineOptions to_options(const updc_options *o) {
     r.autotune = o->autotune;
     r.retune = o->retune;
     r.tune_cache_dir = o->tune_cache_dir ? o->tune_cache_dir : "";
+    r.fft_linear = o->fft_linear;
     return r;
 }
 
@@ -93,6 +94,7 @@ void updc_default_options(updc_options *o) {
     o->autotune = d.autotune;
     o->retune = d.retune;
     o->tune_cache_dir = nullptr;
+    o->fft_linear = d.fft_linear;
 }
 
 int updc_create(const updc_options *opt, updc_engine **out) {

@@ -46,7 +46,7 @@ enum DevErrorCode : uint32_t {
     ERR_LINKMAP_TARGET = 10,         // LinkMap target outside the grid (defensive bounds check)
     ERR_DEVICE_TIMEOUT = 11,         // a bounded device-side wait ran out
 };
-enum DevErrorStage : uint64_t { STAGE_DETECTOR = 1, STAGE_UPDATE = 2, STAGE_SETUP = 3 };
+enum DevErrorStage : uint64_t { STAGE_DETECTOR = 1, STAGE_UPDATE = 2, STAGE_SETUP = 3, STAGE_TRANSFORM = 4 };
 
 __host__ __device__ inline uint64_t make_error_key(uint64_t stage, uint64_t index, uint32_t code) {
     return (stage << 56) | ((index & 0xFFFFFFFFFFull) << 8) | (uint64_t)code;

@@ -637,7 +637,7 @@ template <typename T> class EngineImpl final : public Engine {
     void set_psf(int k, const void *psf, int pw, int phh, int as_double) override {
         if (k < 0 || k >= nexp_) throw Error(1, "exposure index out of range");
         const int tw = transposed_ ? phh : pw, th = transposed_ ? pw : phh;
-        if (pw < 1 || phh < 1 || W_ + tw - 1 > FW_ || H_ + th - 1 > FH_)
+        if (pw < 1 || phh < 1 || min_fft_length(W_, tw) > FW_ || min_fft_length(H_, th) > FH_)
             throw Error(1, "PSF larger than the FFT shape allows");
         const size_t nu = (size_t)M_ + 1;
         cx<T> *rp = scratch_spec(0);
@@ -1114,6 +1114,20 @@ template <typename T> class EngineImpl final : public Engine {
         c.seconds = now_s() - t0;
     }
 
+    // Smallest circular length of one axis for a grid of n pixels and PSFs
+    // of extent f along it.  PSF pixel x sits at circular offset x - f/2
+    // (updc_core.c:814-819), in [-(f/2), f - 1 - f/2].  The forward model
+    // keeps outputs y < n of sum_t x[(y - t) mod F] psf[t] and the adjoint of
+    // sum_t s[(y + t) mod F] psf[t]; with x and s zero beyond n, every index
+    // that wraps lands in the zero padding exactly when F >= n + f/2, and
+    // the PSF does not overlap itself when F >= f.  At that length the kept
+    // window equals the linear convolution's, which the reference computes
+    // with F >= n + f - 1 (updc_core.c:1335-1341); fft_linear keeps that rule.
+    int min_fft_length(int n, int f) const {
+        if (opt_.fft_linear) return n + f - 1;
+        return std::max(n + f / 2, f);
+    }
+
     void choose_fft_shape() {
         int mpw = 0, mph = 0;
         for (auto &e : exps_) {
@@ -1121,9 +1135,9 @@ template <typename T> class EngineImpl final : public Engine {
             mph = std::max(mph, e.psf_height);
         }
         const int pad_w = transposed_ ? mph : mpw, pad_h = transposed_ ? mpw : mph;
-        const int min_w = W_ + pad_w - 1, min_h = H_ + pad_h - 1;
+        const int min_w = min_fft_length(W_, pad_w), min_h = min_fft_length(H_, pad_h);
         if ((opt_.fft_width && (opt_.fft_width < min_w || (opt_.fft_width & 1))) || (opt_.fft_height && opt_.fft_height < min_h))
-            throw Error(1, "FFT shape below the linear-convolution minimum or odd width");
+            throw Error(1, "FFT shape below the minimum length or odd width");
         FftChoice c;
         if (opt_.autotune) {
             const std::string cache = tune_cache_path(min_w, min_h);

@@ -20,12 +20,14 @@ struct EngineOptions {
     int device = 0;
     int reuse_links = 1;      // reuse a valid LinkMap file instead of rebuilding it
     int verbose = 0;
-    int fft_width = 0;        // 0: smallest even 7-smooth width >= W + pw - 1
-    int fft_height = 0;       // 0: smallest 7-smooth height >= H + ph - 1
+    int fft_width = 0;        // 0: smallest even 7-smooth width >= the minimum of the length rule
+    int fft_height = 0;       // 0: smallest 7-smooth height >= the minimum of the length rule
     int stage_timing = 0;     // time each stage with events (no graph)
     int autotune = 0;         // time candidate FFT shapes and radix splits on the device
     int retune = 0;           // ignore a cached autotune result
     std::string tune_cache_dir;  // directory of the autotune cache ("" = no cache)
+    int fft_linear = 0;       // 1: minimum lengths W + pw - 1, H + ph - 1 (the reference's rule);
+                              // 0: W + pw/2, H + ph/2 (the kept window is exactly the same)
 };
 
 // Outcome of the FFT autotuner (or of the fixed choice without it).

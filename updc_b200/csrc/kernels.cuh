@@ -294,9 +294,12 @@ __device__ __forceinline__ void row_c2r_tile(const FftPlan &plan, const cx<T> *_
             for (int bx = 0; bx < nbox; ++bx)
                 tma_load_3d(stage + (size_t)bx * ub * B, imap, &bar, y0 * EW, bx * ub, kexp);
         }
-        if (!mbar_wait_bounded(&bar, 0)) {
+        // every thread's wait is bounded; the block then decides together
+        // (one barrier vote), so either all of it goes on or all of it returns
+        const bool arrived = mbar_wait_bounded(&bar, 0);
+        if (__syncthreads_or(!arrived)) {
             if (threadIdx.x == 0)
-                atomicMin(err, (unsigned long long)make_error_key(STAGE_UPDATE, blockIdx.x, ERR_DEVICE_TIMEOUT));
+                atomicMin(err, (unsigned long long)make_error_key(STAGE_TRANSFORM, blockIdx.x, ERR_DEVICE_TIMEOUT));
             return;
         }
         // pairs (k, M - k): both inputs read into registers, then the tile's

@@ -31,18 +31,46 @@ namespace {
 
 constexpr int MAX_DEVICES = 64;
 std::mutex g_setup_mutex;
-unsigned char *g_scratch_addr[MAX_DEVICES] = {};
+// Per device: the context the address was looked up in, and the address.
+struct ScratchEntry {
+    void *context = nullptr;
+    unsigned char *addr = nullptr;
+};
+ScratchEntry g_scratch[MAX_DEVICES];
 
-// Device address of this device's scratch, looked up on the first call on
-// each device.
-unsigned char *scratch_for(int device) {
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[device]) {
-        void *p = nullptr;
-        UPDC_CUDA(cudaGetSymbolAddress(&p, g_update_scratch));
-        g_scratch_addr[device] = static_cast<unsigned char *>(p);
+// The calling thread's current driver context (cuCtxGetCurrent, reached
+// through the runtime's entry-point query so the library needs no -lcuda).
+void *current_context() {
+    using GetCurrent = int (*)(void **);
+    static GetCurrent get = nullptr;
+    if (!get) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        UPDC_CUDA(cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q));
+        if (!fn || q != cudaDriverEntryPointSuccess) throw Error(-2, "cuCtxGetCurrent is unavailable");
+        get = (GetCurrent)fn;
     }
-    return g_scratch_addr[device];
+    void *ctx = nullptr;
+    if (get(&ctx) != 0) throw Error(-2, "cuCtxGetCurrent failed");
+    return ctx;
+}
+
+// Device address of this device's scratch.  It is looked up on the first
+// call on each device and again whenever the device's context changed since
+// (cudaDeviceReset tears the context down and the module, with its scratch,
+// is loaded anew in the next one), so a stale address is never used.
+unsigned char *scratch_for(int device) {
+    void *ctx = current_context();
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    ScratchEntry &e = g_scratch[device];
+    if (!ctx || !e.addr || e.context != ctx) {
+        void *p = nullptr;
+        // also makes the device's primary context current in this thread
+        UPDC_CUDA(cudaGetSymbolAddress(&p, g_update_scratch));
+        e.addr = static_cast<unsigned char *>(p);
+        e.context = current_context();
+    }
+    return e.addr;
 }
 
 }  // namespace

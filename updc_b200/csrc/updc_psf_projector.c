@@ -22,6 +22,86 @@ static void die(const char *message) {
     exit(EXIT_FAILURE);
 }
 
+/* The manifest format (updc/_engine.py writes it, psf_projector.c reads it):
+ * one job per line, tab-separated "input width height vertices output label",
+ * empty lines and lines starting with '#' ignored; runs of separators count
+ * as one and fields after the sixth are ignored.  The file is read whole,
+ * the lines are counted to size the job array once, then each line is cut
+ * into its fields in place. */
+static char *read_text(const char *path, size_t *len) {
+    FILE *f = fopen(path, "rb");
+    if (!f) die("cannot open PSF projection manifest");
+    size_t cap = 4096, n = 0;
+    char *text = malloc(cap + 1);
+    if (!text) die("out of memory");
+    for (;;) {
+        const size_t got = fread(text + n, 1, cap - n, f);
+        n += got;
+        if (n < cap) break;
+        cap *= 2;
+        char *grown = realloc(text, cap + 1);
+        if (!grown) die("out of memory");
+        text = grown;
+    }
+    fclose(f);
+    text[n] = '\0';
+    *len = n;
+    return text;
+}
+
+static int is_separator(char c) { return c == '\t' || c == '\r'; }
+
+/* Cuts the line at p (NUL-terminated) into at most `want` fields. */
+static int split_fields(char *p, char **field, int want) {
+    int count = 0;
+    while (*p && count < want) {
+        while (*p && is_separator(*p)) ++p;
+        if (!*p) break;
+        field[count++] = p;
+        while (*p && !is_separator(*p)) ++p;
+        if (*p) *p++ = '\0';
+    }
+    return count;
+}
+
+static int copy_path(char *dst, size_t cap, const char *src) {
+    const size_t n = strlen(src);
+    if (n >= cap) return 0;
+    memcpy(dst, src, n + 1);
+    return 1;
+}
+
+static Job *parse_jobs(const char *path, int *njobs) {
+    size_t len = 0;
+    char *text = read_text(path, &len);
+    size_t lines = 1;
+    for (size_t i = 0; i < len; ++i) lines += text[i] == '\n';
+    Job *jobs = calloc(lines, sizeof(Job));
+    if (!jobs) die("out of memory");
+    int n = 0;
+    for (char *line = text; line && *line;) {
+        char *next = strchr(line, '\n');
+        if (next) *next++ = '\0';
+        if (line[0] != '\0' && line[0] != '#') {
+            char *field[6];
+            if (split_fields(line, field, 6) < 6) die("PSF manifest needs input,width,height,vertices,output,label");
+            Job *job = &jobs[n++];
+            if (!copy_path(job->input, sizeof(job->input), field[0]) ||
+                !copy_path(job->vertices, sizeof(job->vertices), field[3]) ||
+                !copy_path(job->output, sizeof(job->output), field[4]))
+                die("PSF manifest path too long");
+            job->width = (int)strtol(field[1], NULL, 10);
+            job->height = (int)strtol(field[2], NULL, 10);
+            if (job->width < 1 || job->height < 1) die("invalid PSF input dimensions");
+        }
+        line = next;
+    }
+    free(text);
+    if (n < 1) die("empty PSF projection manifest");
+    *njobs = n;
+    return jobs;
+}
+
 int main(int argc, char **argv) {
     if (argc == 2 && strcmp(argv[1], "--self-test") == 0) {
         const double quad[8] = {-0.5, -0.5, -0.5, 0.5, 0.5, 0.5, 0.5, -0.5};
@@ -31,38 +111,8 @@ int main(int argc, char **argv) {
         return 0;
     }
     if (argc != 4) die("usage: updc_psf_projector manifest workers results.csv");
-    FILE *f = fopen(argv[1], "r");
-    if (!f) die("cannot open PSF projection manifest");
-    int cap = 16, n = 0;
-    Job *jobs = calloc((size_t)cap, sizeof(Job));
-    char line[8192];
-    while (jobs && fgets(line, sizeof(line), f)) {
-        if (line[0] == '\0' || line[0] == '\n' || line[0] == '#') continue;
-        if (n == cap) {
-            cap *= 2;
-            Job *t = realloc(jobs, (size_t)cap * sizeof(Job));
-            if (!t) die("out of memory expanding jobs");
-            jobs = t;
-            memset(jobs + n, 0, (size_t)(cap - n) * sizeof(Job));
-        }
-        char *save = NULL, *field[6];
-        for (int j = 0; j < 6; ++j) field[j] = strtok_r(j ? NULL : line, "\t\r\n", &save);
-        for (int j = 0; j < 6; ++j)
-            if (!field[j]) die("PSF manifest needs input,width,height,vertices,output,label");
-        Job *job = &jobs[n++];
-        if (strlen(field[0]) >= sizeof(job->input) || strlen(field[3]) >= sizeof(job->vertices) ||
-            strlen(field[4]) >= sizeof(job->output))
-            die("PSF manifest path too long");
-        strcpy(job->input, field[0]);
-        job->width = (int)strtol(field[1], NULL, 10);
-        job->height = (int)strtol(field[2], NULL, 10);
-        strcpy(job->vertices, field[3]);
-        strcpy(job->output, field[4]);
-        if (job->width < 1 || job->height < 1) die("invalid PSF input dimensions");
-    }
-    fclose(f);
-    if (!jobs) die("out of memory");
-    if (n < 1) die("empty PSF projection manifest");
+    int n = 0;
+    Job *jobs = parse_jobs(argv[1], &n);
     for (int i = 0; i < n; ++i) {
         Job *j = &jobs[i];
         char msg[512];

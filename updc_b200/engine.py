@@ -49,7 +49,7 @@ class Engine:
     def __init__(self, form: str = "fp32", device: int = 0, use_graph: bool = True,
                  reuse_links: bool = True, compensated_mu: Optional[bool] = None, verbose: bool = False,
                  fft_shape: Optional[tuple] = None, stage_timing: bool = False, autotune: bool = False,
-                 retune: bool = False, tune_cache_dir: Optional[str] = None):
+                 retune: bool = False, tune_cache_dir: Optional[str] = None, fft_linear: bool = False):
         L = _lib.load()
         opt = _lib.Options()
         L.updc_default_options(ctypes.byref(opt))
@@ -64,6 +64,7 @@ class Engine:
         opt.retune = 1 if retune else 0
         self._cache_dir = str(tune_cache_dir).encode() if tune_cache_dir else None
         opt.tune_cache_dir = self._cache_dir
+        opt.fft_linear = 1 if fft_linear else 0
         if fft_shape:
             opt.fft_width, opt.fft_height = fft_shape
         h = ctypes.c_void_p()
