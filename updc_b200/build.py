@@ -29,7 +29,7 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-r
 # geometry must not contract multiply-adds (bit-exact LinkMaps)
 PER_FILE = {"linkmap.cu": ["-fmad=false"], "projector.cu": ["-fmad=false"]}
 SOURCES = ["linkmap.cu", "engine.cu", "capi.cu", "noalloc.cu", "batch.cu", "projector.cu", "preprocess.cu"]
-HEADERS = ["common.cuh", "fft.cuh", "kernels.cuh", "pointwise.cuh", "engine.cuh", "geometry.cuh", "linkmap.cuh",
+HEADERS = ["common.cuh", "fft.cuh", "fft_ct.cuh", "kernels.cuh", "kernels_ct.cuh", "pointwise.cuh", "engine.cuh", "geometry.cuh", "linkmap.cuh",
            "tma.cuh", "nll.cuh", "preprocess.cuh"]
 
 

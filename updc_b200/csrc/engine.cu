@@ -13,6 +13,7 @@
 #include "engine.cuh"
 #include "fft.cuh"
 #include "kernels.cuh"
+#include "kernels_ct.cuh"
 #include "linkmap.cuh"
 #include "pointwise.cuh"
 #include "nll.cuh"
@@ -805,6 +806,14 @@ template <typename T> class EngineImpl final : public Engine {
     float stage_ms_[8] = {};
 
     FftPlan plan_m_, plan_h_;
+    // Compile-time FP32 iteration kernels (kernels_ct.cuh): the catalog
+    // split of each axis when the axis has one (empty: run-time plans), and
+    // its twiddle table.  plan_m_/plan_h_ then hold a run-time split of the
+    // same length for the setup and batched kernels.
+    std::vector<int> ct_row_rad_, ct_col_rad_;
+    cx<T> *ct_tw_row_ = nullptr, *ct_tw_col_ = nullptr;
+    bool ct_rows() const { return sizeof(T) == 4 && !ct_row_rad_.empty() && use_tma_ && row_b_ == 2; }
+    bool ct_cols() const { return sizeof(T) == 4 && !ct_col_rad_.empty(); }
     cx<T> *post_ = nullptr;
     T *estimate_ = nullptr, *coverage_ = nullptr, *den_ = nullptr, *correction_ = nullptr;
     T *blur_ = nullptr, *wr_ = nullptr, *scatter_ = nullptr, *sci_ = nullptr, *wht_ = nullptr;
@@ -878,7 +887,7 @@ template <typename T> class EngineImpl final : public Engine {
         int rt = 0;
         cudaRuntimeGetVersion(&rt);
         char sig[400];
-        snprintf(sig, sizeof(sig), "%s|sm%d%d|%d SMs|cudart %d|updc_b200 tuner 1", p.name, p.major, p.minor,
+        snprintf(sig, sizeof(sig), "%s|sm%d%d|%d SMs|cudart %d|updc_b200 tuner 2", p.name, p.major, p.minor,
                  p.multiProcessorCount, rt);
         return sig;
     }
@@ -969,7 +978,7 @@ template <typename T> class EngineImpl final : public Engine {
 
     // Times the row transform (R2C of H rows of a W-wide plane into an M-point
     // spectrum) for every split of M; returns the best split and its time.
-    std::pair<std::vector<int>, float> tune_row(int M, const T *plane, cx<T> *spec, int *timed) {
+    std::pair<std::vector<int>, float> tune_row(int M, const T *plane, cx<T> *spec, int ld, int *timed) {
         std::pair<std::vector<int>, float> best{{}, 1e30f};
         const int nu = M + 1, fw = 2 * M;
         int B = std::max(1, std::min(Caps<T>::ROW / M, H_));
@@ -988,7 +997,7 @@ template <typename T> class EngineImpl final : public Engine {
             cx<T> *dtab = dalloc<cx<T>>(tab.size(), nullptr);
             UPDC_CUDA(cudaMemcpy(dtab, tab.data(), tab.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
             plan.tw = dtab;
-            const PlaneLoader<T> ld{plane, W_, 0};
+            const PlaneLoader<T> pl{plane, W_, 0};
             dim3 grid((unsigned)ceil_div(H_, B), 1);
             float ms = 0;
             by_pad(plan.pad_shift, [&](auto P) {
@@ -997,8 +1006,8 @@ template <typename T> class EngineImpl final : public Engine {
                     set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false, PS, BR>, smem);
                     ms = time_launch([&] {
                         k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false, PS, BR>
-                            <<<grid, RowNt<T>::value, smem, stream_>>>(plan, dpost, ld, W_, H_, B, FastDiv((uint32_t)B),
-                                                                       SpecRef{spec, H_, 0}, no_map_);
+                            <<<grid, RowNt<T>::value, smem, stream_>>>(plan, dpost, pl, W_, H_, B, FastDiv((uint32_t)B),
+                                                                       SpecRef{spec, ld, 0}, no_map_);
                     });
                 });
             });
@@ -1006,13 +1015,44 @@ template <typename T> class EngineImpl final : public Engine {
             cudaFree(dtab);
             if (ms < best.second) best = {rad, ms};
         }
+        // the compile-time kernels of the catalog splits of M (FP32; two-row
+        // TMA tiles, as the iteration runs them)
+        if constexpr (sizeof(T) == 4) {
+            if (B == 2 && ld % 2 == 0)
+                for (const auto &rad : ct_catalog_splits(0, M)) {
+                    FftPlan unused;
+                    auto tab = fft_make_table<T>(M, rad, unused);
+                    cx<T> *dtab = dalloc<cx<T>>(tab.size(), nullptr);
+                    UPDC_CUDA(cudaMemcpy(dtab, tab.data(), tab.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
+                    CUtensorMap map;
+                    make_tensor_map_3d(&map, spec, (uint64_t)ld, (uint64_t)M + 1, 1, 2, (uint32_t)row_ubox(M));
+                    const size_t smem = row_tma_smem(2, M, sizeof(cx<float>), 31);
+                    float ms = 1e30f;
+                    ct_row_catalog(rad, [&](auto L) {
+                        tune_row_ct(L, smem);
+                        ms = time_launch([&] { launch_tune_row_ct(L, dpost, plane, dtab, map, smem); });
+                    });
+                    ++*timed;
+                    cudaFree(dtab);
+                    if (ms < best.second) best = {rad, ms};
+                }
+        }
         cudaFree(dpost);
         return best;
+    }
+    template <int... R> void tune_row_ct(CtRadices<R...>, size_t smem) { set_smem(k_row_r2c_ct<256, 2, R...>, smem); }
+    template <int... R>
+    void launch_tune_row_ct(CtRadices<R...>, const cx<T> *post, const T *plane, const cx<T> *tw, const CUtensorMap &map,
+                            size_t smem) {
+        dim3 grid((unsigned)ceil_div(H_, 2), 1);
+        k_row_r2c_ct<256, 2, R...><<<grid, 256, smem, stream_>>>(reinterpret_cast<const cx<float> *>(post),
+                                                                 reinterpret_cast<const float *>(plane), W_, H_, 0,
+                                                                 reinterpret_cast<const cx<float> *>(tw), map);
     }
 
     // Times the column transform (nc columns of length FH, H input rows) for
     // every split of FH; returns the best split and its time per column.
-    std::pair<std::vector<int>, float> tune_col(int FH, int nc, const cx<T> *in, cx<T> *out, int *timed) {
+    std::pair<std::vector<int>, float> tune_col(int FH, int nc, const cx<T> *in, int ld, cx<T> *out, int *timed) {
         std::pair<std::vector<int>, float> best{{}, 1e30f};
         for (const auto &rad : split_candidates(FH)) {
             FftPlan plan;
@@ -1030,12 +1070,12 @@ template <typename T> class EngineImpl final : public Engine {
                 if (FH <= Caps<T>::COL_S) {
                     set_smem(k_col_fft<T, CNT, Caps<T>::COL_S, false, PS>, smem);
                     ms = time_launch([&] {
-                        k_col_fft<T, CNT, Caps<T>::COL_S, false, PS><<<(unsigned)nc, CNT, smem, stream_>>>(plan, in, H_, H_, out, FH, FH);
+                        k_col_fft<T, CNT, Caps<T>::COL_S, false, PS><<<(unsigned)nc, CNT, smem, stream_>>>(plan, in, ld, H_, out, FH, FH);
                     });
                 } else {
                     set_smem(k_col_fft<T, CNT, Caps<T>::COL_L, false, PS>, smem);
                     ms = time_launch([&] {
-                        k_col_fft<T, CNT, Caps<T>::COL_L, false, PS><<<(unsigned)nc, CNT, smem, stream_>>>(plan, in, H_, H_, out, FH, FH);
+                        k_col_fft<T, CNT, Caps<T>::COL_L, false, PS><<<(unsigned)nc, CNT, smem, stream_>>>(plan, in, ld, H_, out, FH, FH);
                     });
                 }
             });
@@ -1043,7 +1083,32 @@ template <typename T> class EngineImpl final : public Engine {
             cudaFree(dtab);
             if (ms / nc < best.second) best = {rad, ms / nc};
         }
+        // the compile-time column kernels of the catalog splits of FH (FP32):
+        // the forward column kernel with no exposures is one transform
+        if constexpr (sizeof(T) == 4) {
+            for (const auto &rad : ct_catalog_splits(1, FH)) {
+                FftPlan unused;
+                auto tab = fft_make_table<T>(FH, rad, unused);
+                cx<T> *dtab = dalloc<cx<T>>(tab.size(), nullptr);
+                UPDC_CUDA(cudaMemcpy(dtab, tab.data(), tab.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
+                float ms = 1e30f;
+                ct_col_catalog(rad, [&](auto L) {
+                    ms = time_launch([&] { launch_tune_col_ct(L, nc, in, ld, out, dtab); });
+                });
+                ++*timed;
+                cudaFree(dtab);
+                if (ms / nc < best.second) best = {rad, ms / nc};
+            }
+        }
         return best;
+    }
+    template <int... R>
+    void launch_tune_col_ct(CtRadices<R...>, int nc, const cx<T> *in, int ld, cx<T> *out, const cx<T> *tw) {
+        const size_t b = (size_t)CtProd<R...>::value * sizeof(cx<float>);
+        set_smem(k_col_forward_ct<CT_COL_NT, R...>, b);
+        k_col_forward_ct<CT_COL_NT, R...><<<(unsigned)nc, CT_COL_NT, b, stream_>>>(
+            reinterpret_cast<const cx<float> *>(in), ld, H_, nullptr, 0, 0, nullptr, 0, 0, 0,
+            reinterpret_cast<cx<float> *>(out), reinterpret_cast<const cx<float> *>(tw));
     }
 
     void autotune_shape(int min_w, int min_h, FftChoice &c) {
@@ -1071,16 +1136,18 @@ template <typename T> class EngineImpl final : public Engine {
         const int hmax = *std::max_element(hc.begin(), hc.end());
         T *plane = dalloc<T>(nout_, nullptr);
         UPDC_CUDA(cudaMemset(plane, 0, nout_ * sizeof(T)));
-        cx<T> *spec = dalloc<cx<T>>((size_t)(mmax + 1) * H_, nullptr);
+        // spectra at the iteration's pitch (even for FP32: TMA strides)
+        const int ld = sizeof(T) == 4 ? (H_ + 1) & ~1 : H_;
+        cx<T> *spec = dalloc<cx<T>>((size_t)(mmax + 1) * ld, nullptr);
         cx<T> *cols = dalloc<cx<T>>((size_t)NC * hmax, nullptr);
-        UPDC_CUDA(cudaMemset(spec, 0, (size_t)(mmax + 1) * H_ * sizeof(cx<T>)));
+        UPDC_CUDA(cudaMemset(spec, 0, (size_t)(mmax + 1) * ld * sizeof(cx<T>)));
         std::map<int, std::pair<std::vector<int>, float>> rows, colsb;
         int timed = 0;
         try {
             for (auto &s : shapes) {
-                if (!rows.count(s.first / 2)) rows[s.first / 2] = tune_row(s.first / 2, plane, spec, &timed);
+                if (!rows.count(s.first / 2)) rows[s.first / 2] = tune_row(s.first / 2, plane, spec, ld, &timed);
                 if (!colsb.count(s.second))
-                    colsb[s.second] = tune_col(s.second, std::min(NC, mmax + 1), spec, cols, &timed);
+                    colsb[s.second] = tune_col(s.second, std::min(NC, mmax + 1), spec, ld, cols, &timed);
             }
         } catch (...) {
             cudaFree(plane), cudaFree(spec), cudaFree(cols);
@@ -1160,14 +1227,52 @@ template <typename T> class EngineImpl final : public Engine {
         M_ = FW_ / 2;
         if (M_ > Caps<T>::ROW) throw Error(1, "FFT width exceeds the row-transform capacity");
         if (FH_ > Caps<T>::COL_L) throw Error(1, "FFT height exceeds the column-transform capacity");
-        if (c.row_radices.empty() && !fft_factor(M_, FFT_RMAX, c.row_radices))
+        // a catalog split (compile-time kernels) is preferred where the length
+        // has one and nothing was tuned; a split that is neither a catalog
+        // entry nor a valid run-time one (non-increasing radices <= 16, e.g.
+        // from another build's cache) is replaced by the greedy split
+        ct_row_rad_.clear();
+        ct_col_rad_.clear();
+        if (sizeof(T) == 4) {
+            if (c.row_radices.empty()) {
+                const auto cs = ct_catalog_splits(0, M_);
+                if (!cs.empty()) c.row_radices = cs[0];
+            }
+            if (c.col_radices.empty()) {
+                const auto cs = ct_catalog_splits(1, FH_);
+                if (!cs.empty()) c.col_radices = cs[0];
+            }
+            if (ct_row_catalog(c.row_radices, [](auto) {})) ct_row_rad_ = c.row_radices;
+            if (ct_col_catalog(c.col_radices, [](auto) {})) ct_col_rad_ = c.col_radices;
+        }
+        auto runtime_split = [](int n, const std::vector<int> &rad) {
+            long p = 1;
+            for (size_t i = 0; i < rad.size(); ++i) {
+                if (rad[i] > FFT_RMAX || (i && rad[i] > rad[i - 1])) return false;
+                p *= rad[i];
+            }
+            return !rad.empty() && p == n;
+        };
+        std::vector<int> gen_row = c.row_radices, gen_col = c.col_radices;
+        if (!runtime_split(M_, gen_row) && !fft_factor(M_, FFT_RMAX, gen_row))
             throw Error(1, "FFT length " + std::to_string(M_) + " is not 7-smooth");
-        if (c.col_radices.empty() && !fft_factor(FH_, FFT_RMAX, c.col_radices))
+        if (!runtime_split(FH_, gen_col) && !fft_factor(FH_, FFT_RMAX, gen_col))
             throw Error(1, "FFT length " + std::to_string(FH_) + " is not 7-smooth");
+        if (ct_row_rad_.empty()) c.row_radices = gen_row;
+        if (ct_col_rad_.empty()) c.col_radices = gen_col;
         choice_ = c;
         // twiddle tables
-        auto tm = fft_make_table<T>(M_, c.row_radices, plan_m_);
-        auto th = fft_make_table<T>(FH_, c.col_radices, plan_h_);
+        auto tm = fft_make_table<T>(M_, gen_row, plan_m_);
+        auto th = fft_make_table<T>(FH_, gen_col, plan_h_);
+        for (int axis = 0; axis < 2; ++axis) {
+            const std::vector<int> &rad = axis ? ct_col_rad_ : ct_row_rad_;
+            if (rad.empty()) continue;
+            FftPlan unused;
+            auto t = fft_make_table<T>(axis ? FH_ : M_, rad, unused);
+            cx<T> *d = alloc<cx<T>>(t.size());
+            UPDC_CUDA(cudaMemcpy(d, t.data(), t.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
+            (axis ? ct_tw_col_ : ct_tw_row_) = d;
+        }
         plan_m_.pad_shift = fft_choose_padding(plan_m_, RowNt<T>::value, Caps<T>::ROW, std::max(1, std::min(2, Caps<T>::ROW / M_)));
         plan_h_.pad_shift = fft_choose_padding(plan_h_, ColNt<T>::value, Caps<T>::COL_S, 1);
         cx<T> *dm = alloc<cx<T>>(tm.size()), *dh = alloc<cx<T>>(th.size());
@@ -1225,6 +1330,11 @@ template <typename T> class EngineImpl final : public Engine {
         while (row_b_ > 2 && row_tma_smem(row_b_, M_, sizeof(cx<T>), plan_m_.pad_shift) > SMEM_LIMIT)
             row_b_ -= EW == 1 ? 2 : 1;
         use_tma_ = (row_b_ * EW) % 2 == 0 && row_tma_smem(row_b_, M_, sizeof(cx<T>), plan_m_.pad_shift) <= SMEM_LIMIT;
+        if (!ct_row_rad_.empty() && !(use_tma_ && row_b_ == 2)) {
+            // the compile-time row kernels take two-row TMA tiles
+            ct_row_rad_.clear();
+            choice_.row_radices.assign(plan_m_.radix, plan_m_.radix + plan_m_.nstage);
+        }
         if (use_tma_) {
             const uint64_t d0 = (uint64_t)ldh_ * EW;
             const uint32_t ub = (uint32_t)row_ubox(M_);
@@ -1297,6 +1407,43 @@ template <typename T> class EngineImpl final : public Engine {
             configure_adjoint<AccF64>();
             configure_adjoint<AccKahan>();
         }
+        if constexpr (sizeof(T) == 4) {
+            if (ct_rows())
+                ct_row_catalog(ct_row_rad_, [&](auto L) {
+                    configure_rows_ct(L);
+                });
+            if (ct_cols())
+                ct_col_catalog(ct_col_rad_, [&](auto L) {
+                    configure_cols_ct(L);
+                });
+        }
+    }
+    size_t ct_row_smem() const { return row_tma_smem(2, M_, sizeof(cx<float>), 31); }
+    template <int... R> void configure_rows_ct(CtRadices<R...>) {
+        set_smem(k_row_r2c_ct<256, 2, R...>, ct_row_smem());
+        set_smem(k_row_c2r_ct<256, 2, R...>, ct_row_smem());
+    }
+    template <int... R> void configure_cols_ct(CtRadices<R...>) {
+        const size_t b = (size_t)FH_ * sizeof(cx<float>);
+        set_smem(k_col_forward_ct<CT_COL_NT, R...>, b);
+        set_smem(k_col_adjoint_ct<AccF64, CT_COL_NT, R...>, b);
+        set_smem(k_col_adjoint_ct<AccKahan, CT_COL_NT, R...>, b);
+        set_smem(k_col_adjoint_ct<AccPlain<float>, CT_COL_NT, R...>, b);
+    }
+    template <int... R>
+    void launch_row_r2c_ct(CtRadices<R...>, const float *plane, int batch, size_t plane_stride, const CUtensorMap &map) {
+        dim3 grid((unsigned)ceil_div(H_, 2), (unsigned)batch);
+        k_row_r2c_ct<256, 2, R...><<<grid, 256, ct_row_smem(), stream_>>>(
+            reinterpret_cast<const cx<float> *>(post_), plane, W_, H_, plane_stride,
+            reinterpret_cast<const cx<float> *>(ct_tw_row_), map);
+        UPDC_CUDA(cudaGetLastError());
+    }
+    template <int... R> void launch_row_c2r_ct(CtRadices<R...>, int batch, float *out, const CUtensorMap &map) {
+        dim3 grid((unsigned)ceil_div(H_, 2), (unsigned)batch);
+        k_row_c2r_ct<256, 2, R...><<<grid, 256, ct_row_smem(), stream_>>>(
+            reinterpret_cast<const cx<float> *>(post_), map, H_, W_, (float)scale_factor(), out, nout_,
+            reinterpret_cast<const cx<float> *>(ct_tw_row_), d_err_);
+        UPDC_CUDA(cudaGetLastError());
     }
     template <class Acc> void configure_adjoint() {
         if constexpr (sizeof(typename Acc::S) > 0) {
@@ -1314,6 +1461,12 @@ template <typename T> class EngineImpl final : public Engine {
     // ------------------------------------------------------------------ launches
     // planes [batch][H][W] -> u-major spectra [batch][M+1][ldh], one launch
     void launch_row_r2c_plane(const T *plane, cx<T> *out, int batch, size_t plane_stride, const CUtensorMap &map) {
+        if constexpr (sizeof(T) == 4) {
+            if (ct_rows()) {
+                ct_row_catalog(ct_row_rad_, [&](auto L) { launch_row_r2c_ct(L, plane, batch, plane_stride, map); });
+                return;
+            }
+        }
         const int B = row_batch();
         dim3 grid((unsigned)ceil_div(H_, B), (unsigned)batch);
         const PlaneLoader<T> ld{plane, W_, plane_stride};
@@ -1334,6 +1487,12 @@ template <typename T> class EngineImpl final : public Engine {
     void launch_col_forward() {
         const size_t nu = (size_t)M_ + 1;
         const size_t ks = nu * FH_, ys = nu * ldh_;
+        if constexpr (sizeof(T) == 4) {
+            if (ct_cols()) {
+                ct_col_catalog(ct_col_rad_, [&](auto L) { launch_col_forward_ct(L); });
+                return;
+            }
+        }
         by_pad(plan_h_.pad_shift, [&](auto P) {
             constexpr int PS = decltype(P)::value;
             if (FH_ <= Caps<T>::COL_S)
@@ -1341,6 +1500,24 @@ template <typename T> class EngineImpl final : public Engine {
             else
                 k_col_forward<T, ColNt<T>::value, Caps<T>::COL_L, ColAux<T>, PS><<<(unsigned)nu, ColNt<T>::value, fwd_smem(), stream_>>>(plan_h_, rx_, ldh_, H_, khat_ + act_k0_ * ks, ks, act_n_, act_y(), ldh_, ys, H_, (int)nu, aux_fwd_);
         });
+        UPDC_CUDA(cudaGetLastError());
+    }
+    template <int... R> void launch_col_forward_ct(CtRadices<R...>) {
+        const size_t nu = (size_t)M_ + 1;
+        const size_t ks = nu * FH_, ys = nu * ldh_;
+        k_col_forward_ct<CT_COL_NT, R...><<<(unsigned)nu, CT_COL_NT, (size_t)FH_ * sizeof(cx<float>), stream_>>>(
+            reinterpret_cast<const cx<float> *>(rx_), ldh_, H_,
+            reinterpret_cast<const cx<float> *>(khat_ + act_k0_ * ks), ks, act_n_,
+            reinterpret_cast<cx<float> *>(act_y()), ldh_, ys, H_, reinterpret_cast<cx<float> *>(aux_fwd_),
+            reinterpret_cast<const cx<float> *>(ct_tw_col_));
+        UPDC_CUDA(cudaGetLastError());
+    }
+    template <class Acc, int... R> void launch_col_adjoint_ct(CtRadices<R...>, const cx<T> *khat, typename Acc::S *aux) {
+        const size_t nu = (size_t)M_ + 1;
+        k_col_adjoint_ct<Acc, CT_COL_NT, R...><<<(unsigned)nu, CT_COL_NT, (size_t)FH_ * sizeof(cx<float>), stream_>>>(
+            reinterpret_cast<const cx<float> *>(act_rs()), ldh_, nu * ldh_, H_,
+            reinterpret_cast<const cx<float> *>(khat + act_k0_ * nu * FH_), nu * FH_, act_n_,
+            reinterpret_cast<cx<float> *>(cr_), ldh_, H_, aux, reinterpret_cast<const cx<float> *>(ct_tw_col_));
         UPDC_CUDA(cudaGetLastError());
     }
     template <class Acc> void ensure_adj_aux() {
@@ -1352,6 +1529,12 @@ template <typename T> class EngineImpl final : public Engine {
         if (adj_aux<Acc>()) {
             if (!aux_adj_) aux_adj_ = alloc<typename Acc::S>(nu * FH_);
             aux = (typename Acc::S *)aux_adj_;
+        }
+        if constexpr (sizeof(T) == 4) {
+            if (ct_cols() && aux) {
+                ct_col_catalog(ct_col_rad_, [&](auto L) { launch_col_adjoint_ct<Acc>(L, khat, aux); });
+                return;
+            }
         }
         const size_t s = adj_smem<Acc>();
         by_pad(plan_h_.pad_shift, [&](auto P) {
@@ -1371,6 +1554,12 @@ template <typename T> class EngineImpl final : public Engine {
         launch_col_adjoint_t<AccPlain<T>>(khat_);
     }
     void launch_row_c2r_batched(const cx<T> *in, int batch, T *out, const CUtensorMap &map) {
+        if constexpr (sizeof(T) == 4) {
+            if (ct_rows()) {
+                ct_row_catalog(ct_row_rad_, [&](auto L) { launch_row_c2r_ct(L, batch, out, map); });
+                return;
+            }
+        }
         const int B = row_batch();
         dim3 grid((unsigned)ceil_div(H_, B), (unsigned)batch);
         const T scale = scale_factor();

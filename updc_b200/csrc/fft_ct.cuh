@@ -36,8 +36,17 @@ __device__ __forceinline__ void ct_stage(cx<T> *buf, const cx<T> *__restrict__ t
     constexpr int K = (TOTAL + NT - 1) / NT;
     constexpr bool LAST_FULL = TOTAL % NT == 0;
     const int tid = threadIdx.x;
+    // v is defined on every path (the zeros of the full rounds are dead
+    // stores): registers defined on only some paths stay live around the
+    // back-edge of any loop that calls the transform, and spill
     cx<T> v[K][R];
     int ob[K];
+#pragma unroll
+    for (int kk = 0; kk < K; ++kk) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[kk][r] = cx<T>{T(0), T(0)};
+        ob[kk] = -1;
+    }
 #pragma unroll
     for (int kk = 0; kk < K; ++kk) {
         const bool full = kk < K - 1 || LAST_FULL;
@@ -101,6 +110,96 @@ struct CtStages<N, BATCH, NT, INV, T, NS, TWOFF, R0, R...> {
 template <int BATCH, int NT, bool INV, typename T, int... R>
 __device__ __forceinline__ void ct_fft(cx<T> *buf, const cx<T> *__restrict__ tw) {
     CtStages<CtProd<R...>::value, BATCH, NT, INV, T, 1, 0, R...>::run(buf, tw);
+}
+
+// ---------------------------------------------------------------------------- edge stages
+// The first stage reads its inputs through `in(row, i)` (element i of
+// sequence row, e.g. straight from global memory) and writes the shared
+// buffer; the last stage reads the shared buffer and hands its outputs to
+// `out(row, i, v)`.  Neither reads and writes the same memory, so each
+// butterfly is loaded, transformed and stored before the next one (no
+// registers held across a barrier), and a transform of S stages makes S - 1
+// shared-memory round trips instead of S + 1.
+//
+// First stage: Ns = 1, no twiddles; butterfly j reads i = j + r N/R and
+// writes j R + s.  Ends with a barrier.
+template <int R, int N, int BATCH, int NT, bool INV, typename T, class In>
+__device__ __forceinline__ void ct_first(const In &in, cx<T> *buf) {
+    constexpr int NB = N / R;
+    constexpr int TOTAL = NB * BATCH;
+    constexpr int K = (TOTAL + NT - 1) / NT;
+#pragma unroll
+    for (int kk = 0; kk < K; ++kk) {
+        const int b = threadIdx.x + kk * NT;
+        if ((kk + 1) * NT <= TOTAL || b < TOTAL) {
+            const int row = BATCH == 1 ? 0 : b / NB;
+            const int j = b - row * NB;
+            cx<T> v[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[r] = in(row, j + r * NB);
+            Dft<R, INV, T>::run(v);
+            cx<T> *dst = buf + row * N + j * R;
+            static_for<0, R>([&](auto p) { dst[Dft<R, INV, T>::out(p)] = v[p]; });
+        }
+    }
+    __syncthreads();
+}
+
+// Last stage: Ns = N/R, so k = j and butterfly j writes i = j + s N/R.
+// Starts from a complete buffer; no barrier at its end.
+template <int R, int TWOFF, int N, int BATCH, int NT, bool INV, typename T, class Out>
+__device__ __forceinline__ void ct_last(const cx<T> *buf, const cx<T> *__restrict__ tw, const Out &out) {
+    constexpr int NB = N / R;
+    constexpr int TOTAL = NB * BATCH;
+    constexpr int K = (TOTAL + NT - 1) / NT;
+#pragma unroll
+    for (int kk = 0; kk < K; ++kk) {
+        const int b = threadIdx.x + kk * NT;
+        if ((kk + 1) * NT <= TOTAL || b < TOTAL) {
+            const int row = BATCH == 1 ? 0 : b / NB;
+            const int j = b - row * NB;
+            cx<T> v[R];
+            const cx<T> *src = buf + row * N + j;
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[r] = src[r * NB];
+            const cx<T> *t = tw + TWOFF + j;
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                cx<T> w = t[(r - 1) * NB];
+                if (INV) w.y = -w.y;
+                v[r] = fmulc(v[r], w);
+            }
+            Dft<R, INV, T>::run(v);
+            static_for<0, R>([&](auto p) { out(row, j + Dft<R, INV, T>::out(p) * NB, v[p]); });
+        }
+    }
+}
+
+template <int N, int BATCH, int NT, bool INV, typename T, int NS, int TWOFF, class Out, int... R> struct CtTail;
+template <int N, int BATCH, int NT, bool INV, typename T, int NS, int TWOFF, class Out, int RL>
+struct CtTail<N, BATCH, NT, INV, T, NS, TWOFF, Out, RL> {
+    __device__ __forceinline__ static void run(cx<T> *buf, const cx<T> *tw, const Out &out) {
+        static_assert(NS * RL == N, "radices must multiply to the length");
+        ct_last<RL, TWOFF, N, BATCH, NT, INV, T>(buf, tw, out);
+    }
+};
+template <int N, int BATCH, int NT, bool INV, typename T, int NS, int TWOFF, class Out, int R0, int R1, int... R>
+struct CtTail<N, BATCH, NT, INV, T, NS, TWOFF, Out, R0, R1, R...> {
+    __device__ __forceinline__ static void run(cx<T> *buf, const cx<T> *tw, const Out &out) {
+        ct_stage<R0, NS, TWOFF, N, BATCH, NT, INV, T>(buf, tw);
+        CtTail<N, BATCH, NT, INV, T, NS * R0, TWOFF + (R0 - 1) * NS, Out, R1, R...>::run(buf, tw, out);
+    }
+};
+
+// Transform of BATCH sequences with at least two stages: inputs through
+// `in`, outputs through `out`, `buf` (BATCH*N complex) as the exchange.
+// The caller synchronises before `buf` is written again.
+template <int BATCH, int NT, bool INV, typename T, int R0, int... R, class In, class Out>
+__device__ __forceinline__ void ct_fft_io(const In &in, cx<T> *buf, const cx<T> *__restrict__ tw, const Out &out) {
+    static_assert(sizeof...(R) >= 1, "at least two stages");
+    constexpr int N = CtProd<R0, R...>::value;
+    ct_first<R0, N, BATCH, NT, INV, T>(in, buf);
+    CtTail<N, BATCH, NT, INV, T, R0, R0 - 1, Out, R...>::run(buf, tw, out);
 }
 
 }  // namespace updc
