@@ -328,11 +328,14 @@ def reference_check(ds, w, form, device, **engine_kw):
             "reference_iteration_ms": [round(1000.0 * v, 1) for v in its], "cores": cores, "fft_workers": fftw}
 
 
-def fp64_comparison(eng, ds, w, args, device):
+def fp64_comparison(eng, ds, w, args, device, **engine_kw):
     """The metric's accuracy side: run the FP64 form (the GPU oracle) on the
     same inputs to the workload's full iteration count, bring the timed engine
     to the same count, and report the relative RMS of x, the FreezeMu masks
-    that differ, and the FP64 form's own device ms/iteration."""
+    that differ, and the FP64 form's own device ms/iteration.  The other FP32
+    forms (Kahan-compensated sums; the reference's plain FP32 arithmetic) run
+    the same count on the same FFT plans and are compared with it the same
+    way (`forms`)."""
     import numpy as np
     from updc_b200.engine import Engine
     done = eng.iterations_done
@@ -344,16 +347,28 @@ def fp64_comparison(eng, ds, w, args, device):
     warm = 3
     st = ref.iterate(target, check_each=False)
     ms64 = 1000.0 * sum(s.seconds for s in st[warm:]) / max(1, target - warm)
-    x32 = eng.plane("estimate", as_double=True)
     x64 = ref.plane("estimate", as_double=True)
-    d = x32 - x64
-    rel_rms = float(np.sqrt(np.mean(d * d) / np.mean(x64 * x64)))
     mask = np.abs(x64) > 1e-8 * np.abs(x64).max()
-    max_rel = float(np.max(np.abs(d[mask]) / np.abs(x64[mask])))
-    mism = sum(int(np.count_nonzero(eng.plane("frozen", k) != ref.plane("frozen", k))) for k in range(w.nexp))
+    frozen64 = [ref.plane("frozen", k) for k in range(w.nexp)]
     ref.close()
-    return {"iterations": target, "rel_rms": rel_rms, "max_rel_masked": max_rel, "frozen_mismatch": mism,
-            "fp64_ms_per_iteration": round(ms64, 4)}
+
+    def against_fp64(e):
+        d = e.plane("estimate", as_double=True) - x64
+        mism = sum(int(np.count_nonzero(e.plane("frozen", k) != frozen64[k])) for k in range(w.nexp))
+        return {"rel_rms": float(np.sqrt(np.mean(d * d) / np.mean(x64 * x64))),
+                "max_rel_masked": float(np.max(np.abs(d[mask]) / np.abs(x64[mask]))), "frozen_mismatch": mism}
+
+    out = {"iterations": target, **against_fp64(eng), "fp64_ms_per_iteration": round(ms64, 4), "forms": {}}
+    for form in ("fp32", "fp32-kahan", "fp32-reference"):
+        if form == args.form:
+            continue
+        e = Engine(form=form, device=device, **engine_kw)
+        e.load(str(ds.manifest), w.W, w.H, w.iw, w.ih, w.nexp).setup()
+        st = e.iterate(target, check_each=False)
+        out["forms"][form] = {**against_fp64(e),
+                              "ms_per_iteration": round(1000.0 * sum(s.seconds for s in st[warm:]) / max(1, target - warm), 4)}
+        e.close()
+    return out
 
 
 def batch_arm(args, rank, world, local_rank):
@@ -568,13 +583,16 @@ def sharded_arm(args, rank, world, local_rank):
         solver = ShardedSolver(shard, dist)
         setup_s = time.time() - t0
         solver.iterate(args.warmup)
+        # one iteration (partial correction, NCCL all-reduce of the engine's
+        # own correction plane, update) as a CUDA graph on the engine's stream
+        solver.capture()
         dist.barrier()
         torch.cuda.synchronize()
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
         with ClockSampler(local_rank) as clocks:
-            ev[0].record()
-            recs = solver.iterate(args.steps)
-            ev[1].record()
+            ev[0].record(shard.stream)
+            recs = solver.iterate(args.steps, records=False)
+            ev[1].record(shard.stream)
             torch.cuda.synchronize()
         t = torch.tensor([ev[0].elapsed_time(ev[1]) / args.steps], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -593,6 +611,7 @@ def sharded_arm(args, rank, world, local_rank):
             eng.read_plane_into("estimate", x)
         te = torch.tensor([1000.0 * (time.time() - t0) / e2e_steps], device="cuda")
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        solver.release()  # the graph holds an NCCL call: released before the group is destroyed
         first, count = shard.first, shard.count
         result = {
             "metric": "ms/iteration", "value": round(ms, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
@@ -600,14 +619,15 @@ def sharded_arm(args, rank, world, local_rank):
             "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32", "data": "synthetic",
             "config": {"workload": args.workload, "form": args.form, "target": [w.W, w.H], "exposures": w.nexp,
                        "detector": [w.iw, w.ih], "psf": w.psf_size, "fft": list(eng.fft_shape),
-                       "parallelism": f"exposure shards over {world} ranks, NCCL all-reduce of the correction plane",
+                       "parallelism": f"exposure shards over {world} ranks, NCCL all-reduce of the correction plane "
+                                      "in place on the engine's stream, one CUDA graph per iteration",
                        "rank0_exposures": [first, first + count],
                        "l2": "working set >> 126 MB L2; no flush needed"},
             "setup_s": round(setup_s, 2),
             "signed_sum_last": recs[-1]["signed_sum"],
             "e2e": {"value": round(float(te.item()), 3), "unit": "ms", "h2d_bytes_per_step": x.nbytes,
                     "d2h_bytes_per_step": x.nbytes},
-            "gpu_launches": (10 + 4) * args.steps,
+            "gpu_launches": (7 if eng.kernel_variants["fused_gather"] else 8) * args.steps,
             "clocks": clocks.summary(),
         }
         if rank == 0:
@@ -635,12 +655,18 @@ def b200_arm(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local_rank))
     w = synth.WORKLOADS[args.workload]
+    if args.exposures:
+        # the workload's geometry with fewer (or more) exposures: a smaller
+        # case of the same kernels for profiler captures
+        import dataclasses
+        w = dataclasses.replace(w, name=f"{w.name}x{args.exposures}", nexp=args.exposures)
     workdir = Path(args.data_dir or tempfile.mkdtemp(prefix=f"updc_bench_r{rank}_"))
-    ds = synth.generate(w.name, workdir, use_torch=True)
+    ds = synth.generate(w, workdir, use_torch=True)
     tune_dir = args.tune_cache or workdir
     if args.tune_cache:
         Path(tune_dir).mkdir(parents=True, exist_ok=True)
-    eng = Engine(form=args.form, device=local_rank, autotune=not args.no_autotune, tune_cache_dir=str(tune_dir))
+    eng = Engine(form=args.form, device=local_rank, autotune=not args.no_autotune and not args.fft_shape,
+                 tune_cache_dir=str(tune_dir), fft_shape=tuple(args.fft_shape) if args.fft_shape else None)
     eng.load(str(ds.manifest), w.W, w.H, w.iw, w.ih, w.nexp)
     t0 = time.time()
     eng.setup()
@@ -668,6 +694,18 @@ def b200_arm(args, rank, world, local_rank):
     links = [(eng.link_count(k), eng.link_encoding(k)) for k in range(w.nexp)]
     sb = stage_bytes(w, fw, fh, links, [L for L, _ in links], 8 if args.form == "fp64" else 4)
     mb = model_bytes(w, fw, fh, links, 8 if args.form == "fp64" else 4)
+    variants = eng.kernel_variants
+    stages = list(STAGES)
+    if variants["fused_gather"]:
+        # one kernel gathers S^T(wr) into the scatter row transform: the two
+        # stages are timed as one, and the scatter plane's write and re-read
+        # (2 x 4 B per target and exposure) no longer exist
+        fused = "gather_scatter_x_pass"
+        stage_ms[fused] = stage_ms.pop("adjoint_gather") + stage_ms.pop("scatter_x_pass")
+        sb[fused] = sb.pop("adjoint_gather") + sb.pop("scatter_x_pass") - 2 * w.nexp * w.W * w.H * (8 if args.form == "fp64" else 4)
+        mb[fused] = mb.pop("adjoint_gather") + mb.pop("scatter_x_pass")
+        i = stages.index("adjoint_gather")
+        stages[i:i + 2] = [fused]
     dom = max(stage_ms, key=stage_ms.get)
     peak, peak_kind = measured_peaks()
     achieved = mb[dom] / (stage_ms[dom] * 1e-3) / 1e9
@@ -691,11 +729,13 @@ def b200_arm(args, rank, world, local_rank):
     nout = w.W * w.H
     fp64 = None
     if args.form != "fp64" and not args.no_fp64_check:
-        fp64 = fp64_comparison(eng, ds, w, args, local_rank)
+        fp64 = fp64_comparison(eng, ds, w, args, local_rank, autotune=not args.no_autotune and not args.fft_shape,
+                               fft_shape=tuple(args.fft_shape) if args.fft_shape else None, tune_cache_dir=str(tune_dir))
     cpu = None
     refcheck = None
     if rank == 0 and world == 1 and not args.no_reference_check:
-        refcheck = reference_check(ds, w, args.form, local_rank, autotune=not args.no_autotune,
+        refcheck = reference_check(ds, w, args.form, local_rank, autotune=not args.no_autotune and not args.fft_shape,
+                                   fft_shape=tuple(args.fft_shape) if args.fft_shape else None,
                                    tune_cache_dir=str(tune_dir))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         its = (refcheck or {}).get("reference_iteration_ms")
@@ -710,9 +750,9 @@ def b200_arm(args, rank, world, local_rank):
         else:
             cpu = cpu_baseline_sample(ds, w)
     # estimate R2C, column forward, forward C2R (all exposures), detector,
-    # adjoint gather, scatter R2C (all exposures), column adjoint, adjoint
-    # C2R, update, reduction
-    launches_per_iter = 10
+    # adjoint gather and scatter R2C (one kernel when fused), column adjoint,
+    # adjoint C2R, update (with its reduction)
+    launches_per_iter = 7 if variants["fused_gather"] else 8
     result = {
         "metric": "ms/iteration", "value": round(ms, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": False,
@@ -729,8 +769,9 @@ def b200_arm(args, rank, world, local_rank):
         "wall_ms_per_step": round(1000.0 * wall / args.steps, 4),
         "setup_s": round(setup_s, 2),
         "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
-        "stage_gbs": {k: round(mb[k] / (stage_ms[k] * 1e-3) / 1e9, 1) for k in STAGES},
-        "stage_gbs_pruned": {k: round(sb[k] / (stage_ms[k] * 1e-3) / 1e9, 1) for k in STAGES},
+        "stage_gbs": {k: round(mb[k] / (stage_ms[k] * 1e-3) / 1e9, 1) for k in stages},
+        "stage_gbs_pruned": {k: round(sb[k] / (stage_ms[k] * 1e-3) / 1e9, 1) for k in stages},
+        "kernel_variants": variants,
         "iteration_model": {"bytes": sum(mb.values()), "achieved_gbs": round(iter_gbs, 1),
                             "frac": round(iter_gbs / peak, 4)},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
@@ -780,6 +821,10 @@ def main():
                    help="smallest 7-smooth FFT shape and greedy radix splits instead of the device autotuner")
     p.add_argument("--no-fp64-check", action="store_true",
                    help="skip the FP64-form run that gives the metric's accuracy side")
+    p.add_argument("--exposures", type=int, default=0,
+                   help="run the workload's geometry with this many exposures (a smaller case for profiling)")
+    p.add_argument("--fft-shape", type=int, nargs=2, default=None, metavar=("FW", "FH"),
+                   help="fixed FFT shape instead of the autotuner's (catalog radix splits where the shape has them)")
     p.add_argument("--no-reference-check", action="store_true",
                    help="skip the full-length run of the reference core that the final x is compared with")
     args = p.parse_args()

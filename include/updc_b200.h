@@ -94,7 +94,9 @@ int updc_write_plane(updc_engine *h, int which, int exposure, const void *host, 
 /* Scalars: 0 weight_scale, 1 max_sensitivity, 2 FFT width, 3 FFT height, 4 masked pixels,
  * 5 working precision bits, 6 compensated raw_mu flag, 7 FFT autotune seconds,
  * 8 FFT plans timed by the autotuner, 9 autotune cache hit, 10 modelled spectral
- * ms per iteration of the tuned choice. */
+ * ms per iteration of the tuned choice, 11 kernel variants of the iteration as
+ * bits (1: row transforms compiled for their radix sequence, 2: column
+ * transforms likewise, 4: adjoint gather fused into the scatter row transform). */
 double updc_scalar(updc_engine *h, int which);
 /* Radix split of an FFT axis (0: the row transform of FW/2 points, 1: the
  * column transform of FH points) in stage order; *count receives the number
@@ -184,6 +186,27 @@ int updc_copy_plane_device(updc_engine *h, int which, int exposure, void *device
  * after the DENOMINATOR plane was replaced. */
 int updc_set_active_exposures(updc_engine *h, int first, int count);
 int updc_refresh_sensitivity(updc_engine *h);
+/* The same exchange without host round trips (no reference counterpart):
+ * updc_plane_device_pointer gives the engine's own device address of a
+ * target plane (ESTIMATE, COVERAGE, DENOMINATOR or CORRECTION: W x H
+ * elements of the form's precision, row-major; valid until updc_destroy) and
+ * updc_engine_stream the CUDA stream every launch of the engine is issued on
+ * (a cudaStream_t).  updc_enqueue_partial enqueues, without waiting, the
+ * partial correction of the active exposures into the CORRECTION plane;
+ * updc_enqueue_update enqueues the update from the CORRECTION plane as it
+ * stands.  A rank sums the CORRECTION plane over ranks in place on the
+ * engine's stream between the two (e.g. an NCCL all-reduce), so the three
+ * steps can also be captured in one CUDA graph.  updc_finish_iteration waits
+ * for the stream, reports a device error recorded by either half like
+ * updc_iterate, and returns the update's signed sum and negative count and
+ * the per-exposure FreezeMu counters (arrays of `exposures` entries; NULL
+ * skips). */
+int updc_plane_device_pointer(updc_engine *h, int which, void **device_ptr);
+int updc_engine_stream(updc_engine *h, void **stream);
+int updc_enqueue_partial(updc_engine *h);
+int updc_enqueue_update(updc_engine *h);
+int updc_finish_iteration(updc_engine *h, double *signed_sum, uint64_t *negative, uint64_t *new_frozen,
+                          uint64_t *total_frozen, double *min_raw_mu);
 
 /* Checkpoint / resume (no reference counterpart: the reference writes the
  * estimate only, core:1460-1470).  updc_save_state writes the estimate and the

@@ -179,12 +179,52 @@ def test_two_row_tiles(engine_lib, oracle, datasets, form, tol, shape):
     assert rel_rms(e2.plane("estimate", as_double=True), s64.estimate) <= 10 * tol
 
 
+@pytest.mark.parametrize("form", ["fp32", "fp32-reference"])
+def test_compile_time_transforms_and_fused_gather(engine_lib, oracle, datasets, form):
+    """A 5040 x 5040 FFT, the shape whose row (2520 = 14 x 12 x 15) and column
+    (5040 = 21 x 16 x 15) transforms are compiled for their radix sequence,
+    and whose iteration gathers S^T(wr) inside the scatter row R2C (no scatter
+    plane).  The forward model against the FP64 oracle; iterations through
+    the fused kernel bit-identical to the stage hooks' separate gather
+    (k_scatter_t) and row R2C; and x after two iterations within 1e-5 of the
+    same form on the default (smallest) shape, since both keep the exact
+    linear convolution."""
+    ds = datasets("c0")
+    w = ds.workload
+    shape = (5040, 5040)
+    a = _engine(ds, form=form, fft_shape=shape, use_graph=False)
+    assert a.fft_shape == shape
+    assert a.fft_radices(0) == [14, 12, 15] and a.fft_radices(1) == [21, 16, 15]
+    s64 = _oracle_solver(oracle, ds, precision=64, fft_shape=shape)
+    x0 = a.plane("estimate")
+    a.set_plane("estimate", s64.estimate)
+    a.stage_forward()
+    for k in (0, w.nexp - 1):
+        assert rel_rms(a.plane("blur", k, as_double=True), s64.forward_blur(k)) <= 2e-6
+    a.set_plane("estimate", x0)
+    b = _engine(ds, form=form, fft_shape=shape, use_graph=False)
+    for it in range(2):
+        a.iterate(1)
+        b.stage_forward()
+        b.stage_detector()
+        b.stage_correction()
+        b.stage_update()
+        np.testing.assert_array_equal(a.plane("estimate"), b.plane("estimate"), err_msg=f"iteration {it + 1}")
+    small = _engine(ds, form=form)
+    assert small.fft_shape != shape
+    small.iterate(2)
+    assert rel_rms(a.plane("estimate"), small.plane("estimate")) <= 1e-5
+    for e in (a, b, small):
+        e.close()
+
+
 # ---------------------------------------------------------------------------- detector / update
-@pytest.mark.parametrize("background", [None, -100.0])
-def test_detector_and_adjoint_gather_bit_exact(engine_lib, oracle, datasets, background):
+@pytest.mark.parametrize("name,background", [("c0", None), ("c0", -100.0), ("abs32", None)])
+def test_detector_and_adjoint_gather_bit_exact(engine_lib, oracle, datasets, name, background):
     """Same blur in, same scatter out: the fused detector loop, FreezeMu and the
-    target-major gather reproduce updc_core.c:1152-1177 bit for bit."""
-    ds = datasets("c0", background)
+    target-major gather reproduce updc_core.c:1152-1177 bit for bit, for a
+    DELTA16 and an ABS32 LinkMap."""
+    ds = datasets(name, background)
     e = _engine(ds, form="fp32-reference")
     s = _oracle_solver(oracle, ds)
     blurs = [s.forward_blur(k) for k in range(ds.workload.nexp)]
@@ -230,14 +270,28 @@ def _reference_run(ref_bin, ds, iterations, tmp_path, prefix="ref"):
 
 @pytest.mark.parametrize("name", ["c0", "medium"])
 def test_fp32_solve_matches_reference(engine_lib, reference_binary, datasets, name, tmp_path):
-    """FP32 form after the workload's iterations within 1e-5 relative RMS of the reference core."""
+    """FP32 form after the workload's iterations within 1e-5 relative RMS of
+    the reference core, with the reference's FreezeMu counts, and the
+    min_raw_mu column of its freeze CSV (updc_core.c:1429, "%.9g" of the
+    FP32 minimum) within 1e-5 relative for both FP32 forms.  The column cannot
+    match byte for byte: raw_mu is a sum over blurred pixels, and this FFT
+    rounds differently from the reference's, so the minima differ in their
+    last bits (the detector itself is bit-exact given the same blur)."""
     ds = datasets(name)
     w = ds.workload
-    xref, _ = _reference_run(reference_binary, ds, w.iterations, tmp_path)
-    e = _engine(ds, form="fp32")
-    e.iterate(w.iterations)
-    x = e.plane("estimate")
-    assert rel_rms(x, xref) <= 1e-5
+    xref, rows = _reference_run(reference_binary, ds, w.iterations, tmp_path)
+    for form in ("fp32", "fp32-reference"):
+        e = _engine(ds, form=form)
+        st = e.iterate(w.iterations)
+        x = e.plane("estimate")
+        if form == "fp32":
+            assert rel_rms(x, xref) <= 1e-5
+        mine = [(int(s.new_frozen[k]), int(s.total_frozen[k]), float(np.float32(s.min_raw_mu[k])))
+                for s in st for k in range(w.nexp)]
+        assert [(a, b) for a, b, _ in mine] == [(int(r["n_new_frozen"]), int(r["n_total_frozen"])) for r in rows]
+        ref_mu = np.array([float(r["min_raw_mu"]) for r in rows])
+        np.testing.assert_allclose(np.array([m for _, _, m in mine]), ref_mu, rtol=1e-5)
+        e.close()
 
 
 def test_fp64_solve_matches_fp64_oracle(engine_lib, oracle, datasets):
@@ -252,7 +306,14 @@ def test_fp64_solve_matches_fp64_oracle(engine_lib, oracle, datasets):
 
 def test_forced_freeze_rows_match_reference(engine_lib, reference_binary, datasets, tmp_path):
     """Background -100 (the reference smoke test's forced FreezeMu): per-iteration
-    freeze counts equal the reference core's and the totals accumulate."""
+    freeze counts equal the reference core's to within 0.1% of the frozen
+    total, and the totals accumulate.  Exact equality is not expected here:
+    with the -100 background many raw_mu sit within FFT rounding of the
+    freeze threshold (raw_mu <= 0), and this FFT rounds differently from the
+    reference's, so a few pixels can freeze one iteration earlier or later.
+    Given the same blur planes the freeze decisions are bit-exact
+    (test_detector_and_adjoint_gather_bit_exact), and on the reference's own
+    forced-freeze fixture the counts match exactly (test_golden)."""
     ds = datasets("c0", -100.0)
     w = ds.workload
     iters = 4

@@ -55,8 +55,10 @@ class ToyShard:
     def broadcast_denominator(self, dist, group=None):
         dist.broadcast(self.D, src=0, group=group)
 
-    def apply_update(self, c):
+    def enqueue_update(self, c):
         self.x = self.x * (c / self.D)
+
+    def finish(self):
         return float(self.x.sum()), int((self.x < 0).sum())
 
 
@@ -106,13 +108,66 @@ def test_two_exposure_shards_match_the_whole_field(engine_lib, datasets, form, t
 
     whole = engine()
     shards = [EngineShard(engine(), *shard_range(w.nexp, r, 2)) for r in range(2)]
+    cur = torch.cuda.current_stream()
     for _ in range(5):
         whole.iterate(1)
-        c = shards[0].partial_correction().clone() + shards[1].partial_correction()
+        parts = [s.partial_correction() for s in shards]   # enqueued on each engine's stream
         for s in shards:
+            cur.wait_stream(s.stream)
+        c = parts[0] + parts[1]                             # the all-reduce of two ranks, on one GPU
+        for s in shards:
+            s.stream.wait_stream(cur)
             s.apply_update(c)
     ref = whole.plane("estimate", as_double=True)
     for s in shards:
         x = s.engine.plane("estimate", as_double=True)
         assert float(np.sqrt(np.mean((x - ref) ** 2) / np.mean(ref ** 2))) <= tol
     np.testing.assert_array_equal(shards[0].engine.plane("estimate"), shards[1].engine.plane("estimate"))
+
+
+def _nccl_single_rank(ds, form, capture):
+    """One NCCL rank holding every exposure: ShardedSolver's iteration (the
+    engine's own correction plane all-reduced in place on the engine's
+    stream between the two non-blocking halves), eager or replayed from one
+    captured CUDA graph."""
+    import datetime
+    import torch.distributed as dist
+    from updc_b200.sharded import ShardedSolver, open_engine_shard
+    w = ds.workload
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        shard = open_engine_shard(str(ds.manifest), w.W, w.H, w.iw, w.ih, w.nexp, 0, 1, form=form)
+        solver = ShardedSolver(shard, dist)
+        if capture:
+            solver.capture()
+        recs = solver.iterate(4)
+        solver.release()
+        x = shard.engine.plane("estimate")
+        shard.engine.close()
+        return x, recs
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("capture", [False, True])
+def test_nccl_shard_iteration_matches_engine(engine_lib, datasets, capture):
+    """With one rank the NCCL sum is the identity, so the sharded iteration
+    (zero-copy correction plane, collective on the engine's stream, and
+    optionally the whole iteration captured in a CUDA graph with the NCCL
+    call) must equal the engine's own iterations bit for bit."""
+    from updc_b200.engine import Engine
+    ds = datasets("c0")
+    w = ds.workload
+    x, recs = _nccl_single_rank(ds, "fp32", capture)
+    e = Engine(form="fp32", use_graph=False)
+    e.load(str(ds.manifest), w.W, w.H, w.iw, w.ih, w.nexp).setup()
+    st = e.iterate(4)
+    np.testing.assert_array_equal(x, e.plane("estimate"))
+    assert [r["signed_sum"] for r in recs] == [s.signed_sum for s in st]
+    assert [r["negative"] for r in recs] == [s.negative for s in st]
+    e.close()

@@ -102,6 +102,11 @@ def load() -> ctypes.CDLL:
     L.updc_batch_iterate.argtypes = [P, c.c_int, c.c_int, P, P, P, P]
     L.updc_set_active_exposures.argtypes = [P, c.c_int, c.c_int]
     L.updc_refresh_sensitivity.argtypes = [P]
+    L.updc_plane_device_pointer.argtypes = [P, c.c_int, c.POINTER(c.c_void_p)]
+    L.updc_engine_stream.argtypes = [P, c.POINTER(c.c_void_p)]
+    L.updc_enqueue_partial.argtypes = [P]
+    L.updc_enqueue_update.argtypes = [P]
+    L.updc_finish_iteration.argtypes = [P, c.POINTER(c.c_double), c.POINTER(c.c_uint64), P, P, P]
     L.updc_save_state.argtypes = [P, c.c_char_p, c.c_uint64]
     L.updc_load_state.argtypes = [P, c.c_char_p, c.POINTER(c.c_uint64)]
     L.updc_link_count.restype = c.c_uint64

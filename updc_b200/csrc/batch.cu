@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
 template <typename T, int NT, int CAP>
 __global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
     kb_col_forward(const FieldDev<T> *__restrict__ F, const int4 *__restrict__ units, int nunits) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ FftPlan s_plan;
     for (int i = blockIdx.x; i < nunits; i += gridDim.x) {
         const int4 u = units[i];
@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
 template <typename T, class Acc, int NT, int CAP>
 __global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
     kb_col_adjoint(const FieldDev<T> *__restrict__ F, const int4 *__restrict__ units, int nunits) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ FftPlan s_plan;
     for (int i = blockIdx.x; i < nunits; i += gridDim.x) {
         const int4 u = units[i];
@@ -122,12 +122,13 @@ __global__ void __launch_bounds__(NT, MinBlocks<NT, CAP, T>::value)
 template <typename T, bool COMP>
 __global__ void __launch_bounds__(DET_WARPS * 32)
     kb_detector(const FieldDev<T> *__restrict__ F, const int4 *__restrict__ units, int nunits) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     for (int i = blockIdx.x; i < nunits; i += gridDim.x) {
         const int4 u = units[i];
         const FieldDev<T> &f = F[u.x];
         const ExpDesc<T> e = f.exps[u.y];
         detector_tiles<T, COMP>(e, u.y, f.nin, f.blur + (size_t)u.y * f.nout, f.wr + (size_t)u.y * f.nin, f.stats,
-                                f.err, (unsigned)u.z, (unsigned)u.w);
+                                f.err, (unsigned)u.z, (unsigned)u.w, smem_raw);
         __syncthreads();
     }
 }
@@ -152,8 +153,8 @@ __global__ void __launch_bounds__(256) kb_update(const FieldDev<T> *__restrict__
     for (int i = blockIdx.x; i < nunits; i += gridDim.x) {
         const int4 u = units[i];
         const FieldDev<T> &f = F[u.x];
-        update_block<T>(f.nout, f.correction, f.den, f.estimate, f.max_sens, f.err, f.part_sum, f.part_neg,
-                        (unsigned)u.y, (unsigned)f.upd_grid);
+        update_block_vec<T>(f.nout, f.correction, f.den, f.estimate, f.max_sens, f.err, f.part_sum, f.part_neg,
+                            (unsigned)u.y, (unsigned)f.upd_grid);
         __syncthreads();
     }
 }
@@ -254,6 +255,8 @@ template <typename T> class BatchImpl final : public Batch {
         build_units();
         if (smem_row_ > SPEC_SMEM_LIMIT || smem_fwd_ > SPEC_SMEM_LIMIT || smem_adj_ > SPEC_SMEM_LIMIT)
             throw Error(1, "batched transforms exceed the shared-memory limit");
+        set_attr(kb_detector<T, true>, sizeof(DetShared));
+        set_attr(kb_detector<T, false>, sizeof(DetShared));
         set_attr(kb_row_r2c<T, SpecRowNt<T>::value, SpecCaps<T>::ROW>, smem_row_);
         set_attr(kb_row_c2r<T, SpecRowNt<T>::value, SpecCaps<T>::ROW>, smem_row_);
         set_attr(kb_col_forward<T, SPEC_NT, SpecCaps<T>::COL_S>, smem_fwd_);
@@ -384,9 +387,9 @@ template <typename T> class BatchImpl final : public Batch {
         kb_col_forward<T, NT, COL><<<grid_for(nunits_[1]), NT, smem_fwd_, stream_>>>(d_fields_, d_units_[1], (int)nunits_[1]);
         kb_row_c2r<T, RNT, ROW><<<grid_for(nunits_[2]), RNT, smem_row_, stream_>>>(d_fields_, d_units_[2], (int)nunits_[2], 0);
         if (comp_mu_)
-            kb_detector<T, true><<<grid_for(nunits_[3]), DET_WARPS * 32, 0, stream_>>>(d_fields_, d_units_[3], (int)nunits_[3]);
+            kb_detector<T, true><<<grid_for(nunits_[3]), DET_WARPS * 32, sizeof(DetShared), stream_>>>(d_fields_, d_units_[3], (int)nunits_[3]);
         else
-            kb_detector<T, false><<<grid_for(nunits_[3]), DET_WARPS * 32, 0, stream_>>>(d_fields_, d_units_[3], (int)nunits_[3]);
+            kb_detector<T, false><<<grid_for(nunits_[3]), DET_WARPS * 32, sizeof(DetShared), stream_>>>(d_fields_, d_units_[3], (int)nunits_[3]);
         kb_scatter<T><<<grid_for(nunits_[4]), 256, 0, stream_>>>(d_fields_, d_units_[4], (int)nunits_[4]);
         kb_row_r2c<T, RNT, ROW><<<grid_for(nunits_[5]), RNT, smem_row_, stream_>>>(d_fields_, d_units_[5], (int)nunits_[5], 1);
         launch_adjoint();

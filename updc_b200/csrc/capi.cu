@@ -273,6 +273,44 @@ int updc_refresh_sensitivity(updc_engine *h) {
         h->e->refresh_sensitivity();
     });
 }
+int updc_plane_device_pointer(updc_engine *h, int which, void **device_ptr) {
+    return guarded([&] {
+        if (!h || !device_ptr) throw Error(1, "null handle or output pointer");
+        *device_ptr = h->e->plane_device(which);
+    });
+}
+int updc_engine_stream(updc_engine *h, void **stream) {
+    return guarded([&] {
+        if (!h || !stream) throw Error(1, "null handle or output pointer");
+        *stream = static_cast<void *>(h->e->stream());
+    });
+}
+int updc_enqueue_partial(updc_engine *h) {
+    return guarded([&] {
+        if (!h) throw Error(1, "null handle");
+        h->e->enqueue_partial();
+    });
+}
+int updc_enqueue_update(updc_engine *h) {
+    return guarded([&] {
+        if (!h) throw Error(1, "null handle");
+        h->e->enqueue_update();
+    });
+}
+int updc_finish_iteration(updc_engine *h, double *sum, uint64_t *neg, uint64_t *nn, uint64_t *nt, double *mn) {
+    return guarded([&] {
+        if (!h) throw Error(1, "null handle");
+        IterationRecord r;
+        h->e->finish_iteration(&r);
+        if (sum) *sum = r.signed_sum;
+        if (neg) *neg = r.negative;
+        for (int k = 0; k < h->nexp; ++k) {
+            if (nn) nn[k] = r.new_frozen[k];
+            if (nt) nt[k] = r.total_frozen[k];
+            if (mn) mn[k] = r.min_raw_mu[k];
+        }
+    });
+}
 
 int updc_save_state(updc_engine *h, const char *path, uint64_t iteration) {
     return guarded([&] {

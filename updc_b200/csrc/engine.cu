@@ -502,6 +502,33 @@ template <typename T> class EngineImpl final : public Engine {
         launch_row_c2r_batched(cr_, 1, correction_, map_cr_);
         UPDC_CUDA(cudaStreamSynchronize(stream_));
     }
+    void *plane_device(int which) override {
+        switch (which) {
+            case PLANE_ESTIMATE: return estimate_;
+            case PLANE_COVERAGE: return coverage_;
+            case PLANE_DENOMINATOR: return den_;
+            case PLANE_CORRECTION: return correction_;
+            default: throw Error(1, "plane has no single device address");
+        }
+    }
+    cudaStream_t stream() const override { return stream_; }
+    void enqueue_partial() override { enqueue_stages([](int) {}, false); }
+    void enqueue_update() override { launch_update(); }
+    void finish_iteration(IterationRecord *rec) override {
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+        check_error();
+        if (!rec) return;
+        std::vector<ExpStats> st(nexp_);
+        UPDC_CUDA(cudaMemcpy(st.data(), d_stats_, nexp_ * sizeof(ExpStats), cudaMemcpyDeviceToHost));
+        rec->new_frozen.clear(); rec->total_frozen.clear(); rec->min_raw_mu.clear();
+        for (int j = 0; j < nexp_; ++j) {
+            rec->new_frozen.push_back(st[j].nnew);
+            rec->total_frozen.push_back(st[j].ntotal);
+            rec->min_raw_mu.push_back(st[j].min_ordered == ~0ull ? INFINITY : ordered_to_double(st[j].min_ordered));
+        }
+        UPDC_CUDA(cudaMemcpy(&rec->signed_sum, d_red_sum_, 8, cudaMemcpyDeviceToHost));
+        UPDC_CUDA(cudaMemcpy(&rec->negative, d_red_neg_, 8, cudaMemcpyDeviceToHost));
+    }
     void stage_update(IterationRecord *rec) override {
         reset_iteration_state();
         launch_update();
@@ -784,6 +811,7 @@ template <typename T> class EngineImpl final : public Engine {
             case 8: return choice_.candidates;
             case 9: return choice_.cache_hit ? 1 : 0;
             case 10: return choice_.predicted_ms;
+            case 11: return (ct_rows() ? 1 : 0) | (ct_cols() ? 2 : 0) | (fused_gather() ? 4 : 0);
             default: return 0;
         }
     }
@@ -826,6 +854,7 @@ template <typename T> class EngineImpl final : public Engine {
     unsigned long long *d_err_ = nullptr, *d_red_neg_ = nullptr, *d_part_neg_ = nullptr;
     double *d_part_sum_ = nullptr, *d_red_sum_ = nullptr;
     int upd_grid_ = 0;
+    unsigned *d_upd_done_ = nullptr;
     T weight_scale_ = 0, max_sens_ = 0;
     uint64_t masked_ = 0;
     void *pinned_ = nullptr;
@@ -1312,8 +1341,13 @@ template <typename T> class EngineImpl final : public Engine {
         khat_ = alloc<cx<T>>(nexp_ * nu * FH_);
         d_exps_ = alloc<ExpDesc<T>>(nexp_);
         d_stats_ = alloc<ExpStats>(nexp_);
+        init_stats_template();
         d_err_ = alloc<unsigned long long>(1);
-        upd_grid_ = grid1d(nout_);
+        // 16-byte accesses (Vec16<T>::n pixels per thread and step), at most
+        // eight 256-thread blocks per SM
+        upd_grid_ = (int)std::max<size_t>(1, std::min<size_t>(ceil_div(nout_ / Vec16<T>::n, 256), 148 * 8));
+        d_upd_done_ = alloc<unsigned>(1);
+        UPDC_CUDA(cudaMemset(d_upd_done_, 0, sizeof(unsigned)));
         d_part_sum_ = alloc<double>(upd_grid_);
         d_part_neg_ = alloc<unsigned long long>(upd_grid_);
         d_red_sum_ = alloc<double>(1);
@@ -1402,6 +1436,8 @@ template <typename T> class EngineImpl final : public Engine {
         });
         set_smem(k_col_fft<T, NT, Caps<T>::COL_S, false>, fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift));
         set_smem(k_col_fft<T, NT, Caps<T>::COL_L, false>, fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift));
+        set_smem(k_detector<T, true>, sizeof(DetShared));
+        set_smem(k_detector<T, false>, sizeof(DetShared));
         configure_adjoint<AccPlain<T>>();
         if (sizeof(T) == 4) {
             configure_adjoint<AccF64>();
@@ -1420,6 +1456,7 @@ template <typename T> class EngineImpl final : public Engine {
     }
     size_t ct_row_smem() const { return row_tma_smem(2, M_, sizeof(cx<float>), 31); }
     template <int... R> void configure_rows_ct(CtRadices<R...>) {
+        set_smem(k_gather_row_r2c_ct<256, R...>, ct_row_smem());
         set_smem(k_row_r2c_ct<256, 2, R...>, ct_row_smem());
         set_smem(k_row_c2r_ct<256, 2, R...>, ct_row_smem());
     }
@@ -1437,6 +1474,20 @@ template <typename T> class EngineImpl final : public Engine {
             reinterpret_cast<const cx<float> *>(post_), plane, W_, H_, plane_stride,
             reinterpret_cast<const cx<float> *>(ct_tw_row_), map);
         UPDC_CUDA(cudaGetLastError());
+    }
+    // S^T of the active exposures gathered straight into their scatter row
+    // R2C (compile-time row transforms only): the scatter plane is not written.
+    template <int... R> void launch_gather_row_r2c_ct(CtRadices<R...>) {
+        dim3 grid((unsigned)ceil_div(H_, 2), (unsigned)act_n_);
+        k_gather_row_r2c_ct<256, R...><<<grid, 256, ct_row_smem(), stream_>>>(
+            reinterpret_cast<const cx<float> *>(post_), reinterpret_cast<const ExpDesc<float> *>(d_exps_ + act_k0_),
+            reinterpret_cast<const float *>(wr_ + (size_t)act_k0_ * nin_), nin_, W_, H_,
+            reinterpret_cast<const cx<float> *>(ct_tw_row_), map_rs_);
+        UPDC_CUDA(cudaGetLastError());
+    }
+    bool fused_gather() const { return ct_rows(); }
+    void launch_gather_scatter_rows() {
+        if constexpr (sizeof(T) == 4) ct_row_catalog(ct_row_rad_, [&](auto L) { launch_gather_row_r2c_ct(L); });
     }
     template <int... R> void launch_row_c2r_ct(CtRadices<R...>, int batch, float *out, const CUtensorMap &map) {
         dim3 grid((unsigned)ceil_div(H_, 2), (unsigned)batch);
@@ -1586,10 +1637,10 @@ template <typename T> class EngineImpl final : public Engine {
         dim3 grid((unsigned)std::min<size_t>(ceil_div(nin_, 256), 148 * 8), (unsigned)act_n_);
         const size_t k0 = act_k0_;
         if (comp_mu_)
-            k_detector<T, true><<<grid, 256, 0, stream_>>>(d_exps_ + k0, nin_, nout_, blur_ + k0 * nout_, wr_ + k0 * nin_,
+            k_detector<T, true><<<grid, 256, sizeof(DetShared), stream_>>>(d_exps_ + k0, nin_, nout_, blur_ + k0 * nout_, wr_ + k0 * nin_,
                                                             d_stats_ + k0, d_err_);
         else
-            k_detector<T, false><<<grid, 256, 0, stream_>>>(d_exps_ + k0, nin_, nout_, blur_ + k0 * nout_, wr_ + k0 * nin_,
+            k_detector<T, false><<<grid, 256, sizeof(DetShared), stream_>>>(d_exps_ + k0, nin_, nout_, blur_ + k0 * nout_, wr_ + k0 * nin_,
                                                              d_stats_ + k0, d_err_);
         UPDC_CUDA(cudaGetLastError());
     }
@@ -1600,53 +1651,63 @@ template <typename T> class EngineImpl final : public Engine {
         UPDC_CUDA(cudaGetLastError());
     }
     void launch_update() {
-        k_update<T><<<upd_grid_, 256, 0, stream_>>>(nout_, correction_, den_, estimate_, max_sens_, d_err_, d_part_sum_, d_part_neg_);
-        k_reduce_partials<<<1, 256, 0, stream_>>>(d_part_sum_, d_part_neg_, upd_grid_, d_red_sum_, d_red_neg_);
+        k_update_vec<T><<<upd_grid_, 256, 0, stream_>>>(nout_, correction_, den_, estimate_, max_sens_, d_err_, d_part_sum_,
+                                                        d_part_neg_, d_upd_done_, d_red_sum_, d_red_neg_);
         UPDC_CUDA(cudaGetLastError());
     }
-    void reset_iteration_state() {
-        // stats: nnew = ntotal = 0, min = ~0
+    // The per-iteration counters' initial values (nnew = ntotal = 0, min =
+    // ~0), kept on the device so that an iteration enqueues only copies
+    // (nothing allocates or waits inside a stream capture).
+    void init_stats_template() {
         static_assert(sizeof(ExpStats) == 32, "ExpStats layout");
         std::vector<ExpStats> init(nexp_);
         for (auto &s : init) { s.nnew = 0; s.ntotal = 0; s.min_ordered = ~0ull; s.pad = 0; }
-        if (!stats_init_) {
-            stats_init_ = alloc<ExpStats>(nexp_);
-            UPDC_CUDA(cudaMemcpy(stats_init_, init.data(), nexp_ * sizeof(ExpStats), cudaMemcpyHostToDevice));
-        }
+        stats_init_ = alloc<ExpStats>(nexp_);
+        UPDC_CUDA(cudaMemcpy(stats_init_, init.data(), nexp_ * sizeof(ExpStats), cudaMemcpyHostToDevice));
+    }
+    void reset_iteration_state() {
         UPDC_CUDA(cudaMemcpyAsync(d_stats_, stats_init_, nexp_ * sizeof(ExpStats), cudaMemcpyDeviceToDevice, stream_));
         UPDC_CUDA(cudaMemsetAsync(d_err_, 0xFF, 8, stream_));
     }
     ExpStats *stats_init_ = nullptr;
 
-    void enqueue_iteration(bool timed) {
-        cudaEvent_t ev[9];
-        if (timed) {
-            for (auto &e : ev) UPDC_CUDA(cudaEventCreate(&e));
-            UPDC_CUDA(cudaEventRecord(ev[0], stream_));
-        }
+    // The launches of one iteration; mark(i) is called at the stage
+    // boundaries (events of the stage timing), the update only with `update`.
+    template <class Mark> void enqueue_stages(const Mark &mark, bool update) {
+        mark(0);
         reset_iteration_state();
         launch_row_r2c_plane(estimate_, rx_, 1, 0, map_rx_);                      // estimate R2C, x pass
-        if (timed) UPDC_CUDA(cudaEventRecord(ev[1], stream_));
+        mark(1);
         launch_col_forward();                                               // y pass + OTF + inverse y pass
-        if (timed) UPDC_CUDA(cudaEventRecord(ev[2], stream_));
+        mark(2);
         launch_row_c2r_batched(act_y(), act_n_, blur_ + (size_t)act_k0_ * nout_, map_y_);  // inverse x pass + crop
-        if (timed) UPDC_CUDA(cudaEventRecord(ev[3], stream_));
+        mark(3);
         launch_detector();                                                  // gather / FreezeMu / ratio
-        if (timed) UPDC_CUDA(cudaEventRecord(ev[4], stream_));
-        launch_scatter(wr_, scatter_);                                      // S^T (transposed gather)
-        if (timed) UPDC_CUDA(cudaEventRecord(ev[5], stream_));
-        launch_row_r2c_plane(scatter_ + (size_t)act_k0_ * nout_, act_rs(), act_n_, nout_, map_rs_);  // scatter R2C, x pass
-        if (timed) UPDC_CUDA(cudaEventRecord(ev[6], stream_));
+        mark(4);
+        if (fused_gather()) {
+            // S^T gathered inside the scatter R2C's x pass (timed as that pass)
+            mark(5);
+            launch_gather_scatter_rows();
+        } else {
+            launch_scatter(wr_, scatter_);                                  // S^T (transposed gather)
+            mark(5);
+            launch_row_r2c_plane(scatter_ + (size_t)act_k0_ * nout_, act_rs(), act_n_, nout_, map_rs_);  // scatter R2C, x pass
+        }
+        mark(6);
         launch_col_adjoint();                                               // y pass, conj-OTF sum, inverse y
         launch_row_c2r_batched(cr_, 1, correction_, map_cr_);                        // inverse x pass + crop
-        if (timed) UPDC_CUDA(cudaEventRecord(ev[7], stream_));
-        launch_update();
-        if (timed) {
-            UPDC_CUDA(cudaEventRecord(ev[8], stream_));
-            UPDC_CUDA(cudaEventSynchronize(ev[8]));
-            for (int s = 0; s < 8; ++s) UPDC_CUDA(cudaEventElapsedTime(&stage_ms_[s], ev[s], ev[s + 1]));
-            for (auto &e : ev) cudaEventDestroy(e);
-        }
+        mark(7);
+        if (update) launch_update();
+        mark(8);
+    }
+    void enqueue_iteration(bool timed) {
+        if (!timed) return enqueue_stages([](int) {}, true);
+        cudaEvent_t ev[9];
+        for (auto &e : ev) UPDC_CUDA(cudaEventCreate(&e));
+        enqueue_stages([&](int i) { UPDC_CUDA(cudaEventRecord(ev[i], stream_)); }, true);
+        UPDC_CUDA(cudaEventSynchronize(ev[8]));
+        for (int s = 0; s < 8; ++s) UPDC_CUDA(cudaEventElapsedTime(&stage_ms_[s], ev[s], ev[s + 1]));
+        for (auto &e : ev) cudaEventDestroy(e);
     }
 
     // One iteration with its events and the copies of its record into

@@ -119,6 +119,22 @@ class Engine {
     // Recompute max_sensitivity from the denominator plane (after it was
     // replaced, e.g. by a sum over shards).
     virtual void refresh_sensitivity() = 0;
+    // Device address of a target plane (estimate, coverage, denominator or
+    // correction: W x H elements of the engine's precision, row-major), valid
+    // while the engine lives, and the stream every launch is issued on.
+    virtual void *plane_device(int which) = 0;
+    virtual cudaStream_t stream() const = 0;
+    // The two halves of an iteration, enqueued on the engine's stream without
+    // waiting, for a caller that puts a collective between them on the same
+    // stream (an exposure shard): the partial correction of the active
+    // exposures (forward model, detector loop, gather, adjoint) into the
+    // correction plane, then the update from the correction plane as it
+    // stands.  finish_iteration waits for the stream, raises a recorded
+    // device error, and fills the FreezeMu counters of every exposure (the
+    // inactive ones zero) and the update's signed sum and negative count.
+    virtual void enqueue_partial() = 0;
+    virtual void enqueue_update() = 0;
+    virtual void finish_iteration(IterationRecord *rec) = 0;
     // Checkpoint / resume: the estimate and the FreezeMu masks with the
     // iteration count they belong to.
     virtual void save_state(const std::string &path, uint64_t iteration) = 0;

@@ -422,7 +422,7 @@ __global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_forw
                                                     const cx<T> *__restrict__ khat, size_t khat_stride, int nexp,
                                                     cx<T> *__restrict__ y, int ldy, size_t y_stride, int rows_out,
                                                     int nu, cx<T> *aux) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     (void)nu;
     col_forward_column<T, NT, CAP, AUX, PADSH>(plan, rx, ldr, rows_in, khat, khat_stride, nexp, y, ldy, y_stride, rows_out,
                                         aux, blockIdx.x, smem_raw);
@@ -516,7 +516,7 @@ template <typename T, class Acc, int NT, int CAP, int AUX = 0, int PADSH = -1>
 __global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_adjoint(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ rs, int ldr, size_t rs_stride,
                                                     int rows_in, const cx<T> *__restrict__ khat, size_t khat_stride, int nexp,
                                                     cx<T> *__restrict__ c, int ldc, int rows_out, typename Acc::S *aux) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     col_adjoint_column<T, Acc, NT, CAP, AUX, PADSH>(plan, rs, ldr, rs_stride, rows_in, khat, khat_stride, nexp, c, ldc,
                                              rows_out, aux, blockIdx.x, smem_raw);
 }
@@ -525,7 +525,7 @@ __global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_adjo
 template <typename T, int NT, int CAP, bool INV, int PADSH = -1>
 __global__ void __launch_bounds__(NT, (MinBlocks<NT, CAP, T>::value)) k_col_fft(const __grid_constant__ FftPlan plan, const cx<T> *__restrict__ in, int ldi, int rows_in,
                                                 cx<T> *__restrict__ out, int ldo, int rows_out) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
     const int n = plan.n, sh = plan_shift<PADSH>(plan);
     const int u = blockIdx.x;

@@ -22,6 +22,7 @@
 
 #include "fft_ct.cuh"
 #include "kernels.cuh"
+#include "pointwise.cuh"
 
 namespace updc {
 
@@ -75,6 +76,114 @@ __global__ void __launch_bounds__(NT, 4)
     const int nb = min(BR, rows - y0);
     const RowPairIn in{planes + kexp * plane_stride + (size_t)y0 * W, W, W, nb, (W & 1) == 0};
     ct_fft_in<BR, NT, false, float, R...>(in, buf, tw);
+    row_r2c_store_tma<float, NT, BR * M, BR>(buf, post, M, 31, BR, nb, FastDiv(), &omap, y0, kexp);
+}
+
+// ---------------------------------------------------------------------------- adjoint gather + row R2C
+// S^T(wr) of targets whose transposed entries are [a[g], b[g]): for each,
+// the ordered chain acc = fmaf(frac, wr[src], acc) over its entries
+// (increasing source pixel, updc_core.c:1173-1176 as seen from the target).
+// The G chains run together, their loads issued in chunks of CH entries.
+template <int CH, int G>
+__device__ __forceinline__ void gather_chains(const ExpDesc<float> &e, const float *__restrict__ wr,
+                                              const uint32_t (&a)[G], const uint32_t (&b)[G], float (&r)[G]) {
+    float acc[G];
+    uint32_t i0[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) acc[g] = 0.f, i0[g] = a[g];
+    bool more = true;
+    while (more) {
+        uint32_t sr[G][CH];
+        float fr[G][CH], v[G][CH];
+#pragma unroll
+        for (int g = 0; g < G; ++g)
+#pragma unroll
+            for (int i = 0; i < CH; ++i) {
+                const bool ok = i0[g] + i < b[g];
+                sr[g][i] = ok ? e.tsrc[i0[g] + i] : 0u;
+                fr[g][i] = ok ? e.tfrac[i0[g] + i] : 0.f;
+            }
+#pragma unroll
+        for (int g = 0; g < G; ++g)
+#pragma unroll
+            for (int i = 0; i < CH; ++i) v[g][i] = i0[g] + i < b[g] ? wr[sr[g][i]] : 0.f;
+        more = false;
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+#pragma unroll
+            for (int i = 0; i < CH; ++i)
+                if (i0[g] + i < b[g]) acc[g] = __fmaf_rn(fr[g][i], v[g][i], acc[g]);
+            i0[g] += CH;
+            more |= i0[g] < b[g];
+        }
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g) r[g] = acc[g];
+}
+
+// Targets a thread gathers together per step of the fused gather.
+#ifndef UPDC_GATHER_TARGETS
+#define UPDC_GATHER_TARGETS 2
+#endif
+
+// Rows [y0, y0 + 2) of exposure blockIdx.y's scatter plane S_k^T(wr_k) are
+// gathered through the target-major map straight into the transform buffer
+// (real row b at floats [b*2M, b*2M + W), zeros up to 2M), so the scatter
+// plane never goes through HBM; then the row R2C of k_row_r2c_ct.  The
+// gathered values are bit-identical to k_scatter_t's (same chain per
+// target).  A thread takes G targets a step (NT apart, so a warp's loads
+// stay coalesced) and loads the next step's CSR offsets before walking this
+// step's entries.
+template <int NT, int... R>
+__global__ void __launch_bounds__(NT, 4)
+    k_gather_row_r2c_ct(const cx<float> *__restrict__ post, const ExpDesc<float> *__restrict__ exps,
+                        const float *__restrict__ wr_all, size_t nin, int W, int rows,
+                        const cx<float> *__restrict__ tw, const __grid_constant__ CUtensorMap omap) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    constexpr int M = CtProd<R...>::value;
+    constexpr int BR = 2, G = UPDC_GATHER_TARGETS;
+    cx<float> *buf = reinterpret_cast<cx<float> *>(smem_raw);
+    float *rowf = reinterpret_cast<float *>(smem_raw);
+    const int y0 = blockIdx.x * BR, kexp = blockIdx.y;
+    const int nb = min(BR, rows - y0);
+    const ExpDesc<float> e = exps[kexp];
+    const float *wr = wr_all + (size_t)kexp * nin;
+    const int count = nb * W;
+    const uint32_t *__restrict__ toff = e.toff + (size_t)y0 * (size_t)W;
+    // CSR offsets of the step at q: targets q + g NT
+    auto offsets = [&](int q, uint32_t (&a)[G], uint32_t (&b)[G]) {
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            const bool h = q + g * NT < count;
+            a[g] = h ? toff[q + g * NT] : 0u;
+            b[g] = h ? toff[q + g * NT + 1] : 0u;
+        }
+    };
+    uint32_t a[G], b[G];
+    offsets(threadIdx.x, a, b);
+    for (int q = threadIdx.x; q < count; q += G * NT) {
+        uint32_t na[G], nb_[G];
+        offsets(q + G * NT, na, nb_);  // in flight during this step's walk
+        float r[G];
+        gather_chains<4, G>(e, wr, a, b, r);
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            const int qg = q + g * NT;
+            if (qg < count) {
+                const int c = qg >= W ? 1 : 0;
+                rowf[c * 2 * M + qg - c * W] = r[g];
+            }
+            a[g] = na[g];
+            b[g] = nb_[g];
+        }
+    }
+    // zero padding of the rows (and the whole of a missing second row)
+    for (int rb = 0; rb < BR; ++rb) {
+        const int x0 = rb < nb ? W : 0;
+        for (int x = x0 + threadIdx.x; x < 2 * M; x += NT) rowf[rb * 2 * M + x] = 0.f;
+    }
+    __syncthreads();
+    ct_fft<BR, NT, false, float, R...>(buf, tw);
     row_r2c_store_tma<float, NT, BR * M, BR>(buf, post, M, 31, BR, nb, FastDiv(), &omap, y0, kexp);
 }
 
@@ -162,15 +271,46 @@ __global__ void __launch_bounds__(NT, 4)
 }
 
 // ---------------------------------------------------------------------------- columns
-constexpr int CT_COL_NT = 384;
+// Threads of the compile-time column kernels (three blocks per SM).
+#ifndef UPDC_CT_COL_NT
+#define UPDC_CT_COL_NT 384
+#endif
+constexpr int CT_COL_NT = UPDC_CT_COL_NT;
+
+// Element v = threadIdx.x + j*NT (j < ceil(N/NT)) of a column, visited in
+// batches of B: the loads of a batch are issued before any of its results
+// is used, so a thread keeps B independent global accesses in flight instead
+// of one at a time.
+template <int N, int NT, int B, class F> __device__ __forceinline__ void column_batches(const F &f) {
+    constexpr int KE = (N + NT - 1) / NT;
+#pragma unroll
+    for (int j0 = 0; j0 < KE; j0 += B) f(j0);
+}
+template <int N, int NT> __device__ __forceinline__ bool column_has(int j) {
+    constexpr int KE = (N + NT - 1) / NT;
+    return j < KE && (N % NT == 0 || (int)threadIdx.x + j * NT < N);
+}
+
+// buf[v] = load(v) over the column, B loads in flight per thread.
+template <int N, int NT, int B, class Load> __device__ __forceinline__ void stage_column(cx<float> *buf, const Load &load) {
+    column_batches<N, NT, B>([&](int j0) {
+        cx<float> t[B];
+#pragma unroll
+        for (int j = 0; j < B; ++j)
+            if (column_has<N, NT>(j0 + j)) t[j] = load((int)threadIdx.x + (j0 + j) * NT);
+#pragma unroll
+        for (int j = 0; j < B; ++j)
+            if (column_has<N, NT>(j0 + j)) buf[threadIdx.x + (j0 + j) * NT] = t[j];
+    });
+}
 
 // Column forward model: transform 0 is FFT(pad(rx[u])) -> X-hat (global
 // scratch, L2-resident); transform it >= 1 is IFFT(X-hat * K_{it-1}) for
 // rows < rows_out, computed as conj(FFT(conj(.))).  Every transform's input
-// is staged in shared memory by all threads together (the product's two
-// loads per element in flight at once), the stages run in place, and the last
-// one writes X-hat or the cropped output straight to global memory.  One
-// transform call site, so one inlined copy of the stages.
+// is staged in shared memory by all threads together (seven elements' loads
+// in flight per thread), the stages run in place, and the last one writes
+// X-hat or the cropped output straight to global memory.  One transform call
+// site, so one inlined copy of the stages.
 struct ColForwardOut {
     cx<float> *dst;
     int lim;
@@ -189,20 +329,20 @@ __global__ void __launch_bounds__(NT, 3)
     constexpr int N = CtProd<R...>::value;
     cx<float> *buf = reinterpret_cast<cx<float> *>(smem_raw);
     const int u = blockIdx.x;
-    cx<float> *xh = aux + (size_t)u * N;
+    cx<float> *__restrict__ xh = aux + (size_t)u * N;
 #pragma unroll 1
     for (int it = 0; it <= nexp; ++it) {
         // the OTF column of the next exposure is fetched into L2 during this transform
         if (threadIdx.x == 0 && it < nexp) prefetch_l2(khat + it * khat_stride + (size_t)u * N, (size_t)N * sizeof(cx<float>));
         if (it == 0) {
-            const cx<float> *src = rx + (size_t)u * ldr;
-            for (int v = threadIdx.x; v < N; v += NT) buf[v] = v < rows_in ? src[v] : cx<float>{0.f, 0.f};
+            const cx<float> *__restrict__ src = rx + (size_t)u * ldr;
+            stage_column<N, NT, 7>(buf, [&](int v) { return v < rows_in ? src[v] : cx<float>{0.f, 0.f}; });
         } else {
-            const cx<float> *kr = khat + (it - 1) * khat_stride + (size_t)u * N;
-            for (int v = threadIdx.x; v < N; v += NT) {
+            const cx<float> *__restrict__ kr = khat + (it - 1) * khat_stride + (size_t)u * N;
+            stage_column<N, NT, 7>(buf, [&](int v) {
                 const cx<float> p = cmul(xh[v], kr[v]);
-                buf[v] = {p.x, -p.y};
-            }
+                return cx<float>{p.x, -p.y};
+            });
         }
         __syncthreads();
         const ColForwardOut out{it == 0 ? xh : y + (it - 1) * y_stride + (size_t)u * ldy, it == 0 ? N : rows_out,
@@ -213,30 +353,17 @@ __global__ void __launch_bounds__(NT, 3)
 }
 
 // Column adjoint: C[u] = IFFT( sum_k conj(K_k[u]) * FFT(pad(Rs_k[u])) ) for
-// rows < rows_out; the sum is taken in exposure order in the column's
-// accumulator (global scratch of Acc::S), the first exposure's product
-// written over whatever the scratch held.
-template <class Acc> struct ColAdjointIO {
-    const cx<float> *src;   // scatter spectrum column of the current exposure
-    const cx<float> *kr;    // K column of the current exposure
-    typename Acc::S *acc;
-    cx<float> *dst;
-    int rows_in, rows_out, phase;  // 0: first exposure, 1: later exposures, 2: the inverse of the sum
+// rows < rows_out.  Each exposure's transform reads its first stage straight
+// from the scatter spectrum and ends in shared memory; the conj-OTF product
+// is then added into the column's accumulator (global scratch of Acc::S, in
+// exposure order, the first exposure's product written over whatever the
+// scratch held) with four elements' accumulator and OTF loads in flight per
+// thread.  Finally the sum is staged back and inverse-transformed.
+struct ColIn {
+    const cx<float> *src;
+    int rows_in;
     __device__ __forceinline__ cx<float> operator()(int, int i) const {
-        if (phase < 2) return i < rows_in ? src[i] : cx<float>{0.f, 0.f};
-        const cx<float> a = Acc::get(acc[i]);
-        return {a.x, -a.y};
-    }
-    __device__ __forceinline__ void operator()(int, int i, cx<float> v) const {
-        if (phase < 2) {
-            typename Acc::S s;
-            if (phase == 0) Acc::zero(s);
-            else s = acc[i];
-            Acc::add(s, v, kr[i]);
-            acc[i] = s;
-        } else if (i < rows_out) {
-            dst[i] = {v.x, -v.y};
-        }
+        return i < rows_in ? src[i] : cx<float>{0.f, 0.f};
     }
 };
 
@@ -247,21 +374,42 @@ __global__ void __launch_bounds__(NT, 3)
                      int ldc, int rows_out, typename Acc::S *__restrict__ aux, const cx<float> *__restrict__ tw) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     constexpr int N = CtProd<R...>::value;
+    constexpr int B = 4;
     cx<float> *buf = reinterpret_cast<cx<float> *>(smem_raw);
     const int u = blockIdx.x;
-    ColAdjointIO<Acc> io{nullptr, nullptr, aux + (size_t)u * N, c + (size_t)u * ldc, rows_in, rows_out, 0};
+    typename Acc::S *__restrict__ acc = aux + (size_t)u * N;
 #pragma unroll 1
-    for (int it = 0; it <= nexp; ++it) {
-        if (it < nexp) {
-            io.src = rs + it * rs_stride + (size_t)u * ldr;
-            io.kr = khat + it * khat_stride + (size_t)u * N;
-            io.phase = it == 0 ? 0 : 1;
-        } else {
-            io.phase = 2;
-        }
-        ct_fft_io<1, NT, false, float, R...>(io, buf, tw, io);
-        __syncthreads();  // buf and the accumulator are read by the next transform
+    for (int it = 0; it < nexp; ++it) {
+        ct_fft_in<1, NT, false, float, R...>(ColIn{rs + it * rs_stride + (size_t)u * ldr, rows_in}, buf, tw);
+        const cx<float> *__restrict__ kr = khat + it * khat_stride + (size_t)u * N;
+        const bool first = it == 0;
+        column_batches<N, NT, B>([&](int j0) {
+            typename Acc::S s[B];
+            cx<float> k[B];
+#pragma unroll
+            for (int j = 0; j < B; ++j)
+                if (column_has<N, NT>(j0 + j)) {
+                    const int v = threadIdx.x + (j0 + j) * NT;
+                    k[j] = kr[v];
+                    if (first) Acc::zero(s[j]);
+                    else s[j] = acc[v];
+                }
+#pragma unroll
+            for (int j = 0; j < B; ++j)
+                if (column_has<N, NT>(j0 + j)) {
+                    const int v = threadIdx.x + (j0 + j) * NT;
+                    Acc::add(s[j], buf[v], k[j]);
+                    acc[v] = s[j];
+                }
+        });
+        __syncthreads();  // buf is rewritten by the next transform
     }
+    stage_column<N, NT, B>(buf, [&](int v) {
+        const cx<float> a = Acc::get(acc[v]);
+        return cx<float>{a.x, -a.y};
+    });
+    __syncthreads();
+    ct_fft_out<1, NT, false, float, R...>(buf, tw, ColForwardOut{c + (size_t)u * ldc, rows_out, -1.f});
 }
 
 // ---------------------------------------------------------------------------- catalog

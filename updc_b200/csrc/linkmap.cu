@@ -116,16 +116,16 @@ bool linkmap_load(const std::string &path, size_t nin, int W, int H, DevLinkMap 
         out.base = dev_alloc<uint32_t>(nin);
         UPDC_CUDA(cudaMemcpyAsync(out.base, host + pos, nin * 4, cudaMemcpyHostToDevice, s));
         pos += nin * 4;
-        out.delta = dev_alloc<uint16_t>(h.nlinks);
+        out.delta = dev_alloc<uint16_t>(h.nlinks + 8);  // 16 bytes of slack: whole-vector loads
         UPDC_CUDA(cudaMemcpyAsync(out.delta, host + pos, h.nlinks * 2, cudaMemcpyHostToDevice, s));
         pos += h.nlinks * 2;
         pos = ((pos + sizeof(h) + 3) & ~(size_t)3) - sizeof(h);
     } else {
-        out.tgt = dev_alloc<uint32_t>(h.nlinks);
+        out.tgt = dev_alloc<uint32_t>(h.nlinks + 4);  // 16 bytes of slack: whole-vector loads
         UPDC_CUDA(cudaMemcpyAsync(out.tgt, host + pos, h.nlinks * 4, cudaMemcpyHostToDevice, s));
         pos += h.nlinks * 4;
     }
-    out.frac = dev_alloc<float>(h.nlinks);
+    out.frac = dev_alloc<float>(h.nlinks + 4);  // 16 bytes of slack: whole-vector loads
     UPDC_CUDA(cudaMemcpyAsync(out.frac, host + pos, h.nlinks * 4, cudaMemcpyHostToDevice, s));
     UPDC_CUDA(cudaStreamSynchronize(s));  // the staging buffer is reused by the next call
     return true;

@@ -2,10 +2,12 @@
 // its scratch (per-block partial sums, the device error record and the two
 // reduced results) lives in one file-scope __device__ array.
 //
-// The kernels are the engine's own update kernels (pointwise.cuh k_update and
-// k_reduce_partials, updc/c_core/updc_core.c:1437-1456) launched with the same
-// grid as the engine's update stage, so the estimate, the signed sum and the
-// negative count are the ones updc_stage_update gives for the same planes.
+// The kernels (pointwise.cuh k_update and k_reduce_partials,
+// updc/c_core/updc_core.c:1437-1456) apply the engine update stage's per-pixel
+// arithmetic, so the estimate and the negative count are the ones
+// updc_stage_update gives for the same planes; the signed sum is the same
+// double-precision sum taken over a different grouping of partial sums (it
+// agrees to rounding).  Caller planes need no particular alignment.
 #include <mutex>
 
 #include "../../include/updc_b200.h"

@@ -180,6 +180,14 @@ class Engine:
                 "modelled_ms": self.scalar(10)}
 
     @property
+    def kernel_variants(self) -> dict:
+        """Which specialised kernels the iteration runs: row / column transforms
+        compiled for their radix sequence, and the adjoint gather fused into
+        the scatter row transform (no scatter plane)."""
+        v = int(self.scalar(11))
+        return {"compiled_rows": bool(v & 1), "compiled_columns": bool(v & 2), "fused_gather": bool(v & 4)}
+
+    @property
     def masked_pixels(self) -> int:
         return int(self.scalar(4))
 
@@ -227,6 +235,42 @@ class Engine:
 
     def refresh_sensitivity(self) -> None:
         check(self._L.updc_refresh_sensitivity(self._h))
+
+    def plane_device_pointer(self, name: str) -> int:
+        """The engine's own device address of a target plane (W x H elements
+        of the form's precision), valid until close()."""
+        p = ctypes.c_void_p()
+        check(self._L.updc_plane_device_pointer(self._h, PLANES[name], ctypes.byref(p)))
+        return int(p.value or 0)
+
+    def stream_handle(self) -> int:
+        """The cudaStream_t every launch of the engine is issued on."""
+        p = ctypes.c_void_p()
+        check(self._L.updc_engine_stream(self._h, ctypes.byref(p)))
+        return int(p.value or 0)
+
+    def enqueue_partial(self) -> None:
+        """Partial correction of the active exposures into the correction
+        plane, enqueued on the engine's stream without waiting."""
+        check(self._L.updc_enqueue_partial(self._h))
+
+    def enqueue_update(self) -> None:
+        """The update from the correction plane as it stands, enqueued on the
+        engine's stream without waiting."""
+        check(self._L.updc_enqueue_update(self._h))
+
+    def finish_iteration(self):
+        """Waits for the engine's stream; returns (signed_sum, negative,
+        new_frozen, total_frozen, min_raw_mu) of the iteration just enqueued."""
+        s = ctypes.c_double()
+        n = ctypes.c_uint64()
+        new = np.zeros(self.nexp, np.uint64)
+        tot = np.zeros(self.nexp, np.uint64)
+        mn = np.zeros(self.nexp, np.float64)
+        check(self._L.updc_finish_iteration(self._h, ctypes.byref(s), ctypes.byref(n), new.ctypes.data,
+                                            tot.ctypes.data, mn.ctypes.data))
+        self.iterations_done += 1
+        return float(s.value), int(n.value), new, tot, mn
 
     # ------------------------------------------------------------------ differentiable model
     def set_exposure_offsets(self, exposure: int, background: float, pedestal: float) -> None:
