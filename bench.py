@@ -154,13 +154,15 @@ def model_bytes(w, fw, fh, links, dtype_bytes=4):
     }
 
 
-# DRAM bytes (read + write) over algorithmic bytes per spectral stage, from
-# the full-set ncu capture of the same kernels on c3 (4 x 1024^2 -> 2048^2,
-# FFT 3584^2): the kernels' traffic grows in proportion to the columns, rows
-# and exposures they process, so this ratio carries a capture of the small
-# case to the benchmark's workload.
-TRAFFIC_RATIO_C3 = {"estimate_x_pass": 21.0 / 46.2, "forward_y_passes": 385.3 / 352.5, "forward_x_pass": 158.9 / 184.6,
-                    "scatter_x_pass": 150.9 / 184.6, "adjoint_y_x_passes": (443.1 + 29.7) / (352.5 + 46.2)}
+# DRAM bytes (read + write) over the bytes each kernel must move, per
+# stage, from the full-set ncu capture of the same kernels on the c1
+# geometry with 2 exposures (profiles/kernels_c1x2_fp32_fullset.md): the
+# kernels' traffic grows in proportion to the rows, columns and exposures
+# they process, so this ratio carries the small case to the benchmark.
+TRAFFIC_RATIO_C1X2 = {"estimate_x_pass": 120.8 / 149.7, "forward_y_passes": 514.8 / 451.0,
+                      "forward_x_pass": 263.1 / 299.4, "detector": 759.5 / 771.6,
+                      "gather_scatter_x_pass": 949.9 / 936.8,
+                      "adjoint_y_x_passes": (620.8 + 114.0) / (451.0 + 149.7), "update": 214.2 / 268.4}
 
 STAGES = ["estimate_x_pass", "forward_y_passes", "forward_x_pass", "detector", "adjoint_gather",
           "scatter_x_pass", "adjoint_y_x_passes", "update"]
@@ -779,8 +781,9 @@ def b200_arm(args, rank, world, local_rank):
                      "algorithmic_bytes": mb[dom],
                      "pruned_bytes": sb[dom], "achieved_pruned": round(achieved_pruned, 1),
                      "frac_pruned": round(achieved_pruned / peak, 4),
-                     "traffic": round(sb[dom] * TRAFFIC_RATIO_C3[dom]) if dom in TRAFFIC_RATIO_C3 else None,
-                     "traffic_source": "ncu dram__bytes_read+write of the c3 capture, scaled by units processed"},
+                     "traffic": round(sb[dom] * TRAFFIC_RATIO_C1X2[dom]) if dom in TRAFFIC_RATIO_C1X2 else None,
+                     "traffic_source": "ncu dram__bytes_read+write of the same kernel on the c1 geometry with 2 "
+                                       "exposures, scaled by the units processed"},
         "cpu_baseline": cpu,
         "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": x.itemsize * nout,
                 "d2h_bytes_per_step": x.itemsize * nout},

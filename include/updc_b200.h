@@ -317,6 +317,13 @@ int updc_robust_background(const float *science, const uint8_t *base_valid, int6
 float updc_polygon_area(const double *xy, int count);
 float updc_overlap_area(const double *quad8, int x, int y);
 int updc_self_test(char *message, size_t capacity);
+/* Device-side failure detection check (no reference counterpart): runs, on
+ * the current device, a bounded mbarrier wait that nothing completes (no copy
+ * is issued), polled at most `polls` times per thread.  It returns status 1
+ * with updc_last_error() = "device wait timed out" once the wait ran out and
+ * the kernel returned (the path a stuck TMA tile of the row transforms
+ * takes); the context stays usable. */
+int updc_device_wait_check(uint32_t polls);
 
 /* The 18-argument solve with status return (no exit): writes <prefix>_NN.bin,
  * <prefix>_mufreeze.csv, <prefix>_timing.csv and the WHT file exactly where the

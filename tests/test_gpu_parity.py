@@ -43,6 +43,23 @@ def test_self_test_on_device(engine_lib):
     assert "OK" in self_test()
 
 
+def test_bounded_device_wait_times_out_and_context_stays_usable(engine_lib, datasets):
+    """Failure detection without a fault: a bounded mbarrier wait that nothing
+    completes (no copy issued) runs out, the block returns together and the
+    host raises "device wait timed out"; the context stays usable, so an
+    engine solve afterwards runs normally."""
+    from updc_b200 import _lib
+    from updc_b200.engine import UpdcError
+    L = _lib.load()
+    for polls in (1, 1000):
+        with pytest.raises(UpdcError, match="device wait timed out"):
+            _lib.check(L.updc_device_wait_check(polls))
+    e = _engine(datasets("small"))
+    st = e.iterate(2)
+    assert len(st) == 2 and np.isfinite(e.plane("estimate")).all()
+    e.close()
+
+
 @pytest.mark.parametrize("name", ["small", "abs32", "c0", "medium"])
 def test_linkmap_build_byte_identical(engine_lib, oracle, datasets, name, tmp_path):
     from updc_b200.engine import build_linkmap

@@ -388,6 +388,10 @@ int updc_self_test(char *msg, size_t cap) {
     return rc;
 }
 
+int updc_device_wait_check(uint32_t polls) {
+    return guarded([&] { device_wait_check(polls); });
+}
+
 // ---------------------------------------------------------------------------- batched fields
 int updc_batch_create(const updc_options *opt, updc_batch **out) {
     return guarded([&] {

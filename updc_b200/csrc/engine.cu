@@ -2099,6 +2099,43 @@ template <typename T> class EngineImpl final : public Engine {
 
 }  // namespace
 
+// ---------------------------------------------------------------------------- wait-timeout check
+// A bounded mbarrier wait that must run out: thread 0 arms the barrier with
+// an expected transaction count that no copy will ever deliver (nothing is
+// issued, so nothing is in flight), every thread polls it at most `polls`
+// times, and the block decides together (as the row kernels do) to record
+// ERR_DEVICE_TIMEOUT and return.  The same path a stuck TMA tile takes.
+__global__ void k_wait_timeout_probe(uint32_t polls, unsigned long long *err) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_arrive_expect_tx(&bar, 16);
+    }
+    __syncthreads();
+    const bool arrived = mbar_wait_bounded(&bar, 0, polls);
+    if (__syncthreads_or(!arrived)) {
+        if (threadIdx.x == 0) atomicMin(err, (unsigned long long)make_error_key(STAGE_TRANSFORM, 0, ERR_DEVICE_TIMEOUT));
+        return;
+    }
+}
+
+void device_wait_check(uint32_t polls) {
+    unsigned long long *err = nullptr;
+    cudaStream_t s = nullptr;
+    UPDC_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    UPDC_CUDA(cudaMalloc(&err, 8));
+    unsigned long long key = ~0ull;
+    UPDC_CUDA(cudaMemsetAsync(err, 0xFF, 8, s));
+    k_wait_timeout_probe<<<1, 32, 0, s>>>(polls, err);
+    cudaError_t rc = cudaGetLastError();
+    if (rc == cudaSuccess) rc = cudaMemcpyAsync(&key, err, 8, cudaMemcpyDeviceToHost, s);
+    if (rc == cudaSuccess) rc = cudaStreamSynchronize(s);
+    cudaFree(err);
+    cudaStreamDestroy(s);
+    UPDC_CUDA(rc);
+    if (key != ~0ull) throw Error(1, error_message((uint32_t)(key & 0xFF)));
+}
+
 std::unique_ptr<Engine> make_engine(const EngineOptions &opt) {
     if (opt.form == FORM_FP64) return std::unique_ptr<Engine>(new EngineImpl<double>(opt));
     return std::unique_ptr<Engine>(new EngineImpl<float>(opt));

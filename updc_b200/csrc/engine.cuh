@@ -186,6 +186,11 @@ class Batch {
 };
 std::unique_ptr<Batch> make_batch(const EngineOptions &opt);
 
+// Runs a device wait that runs out after `polls` polls of an mbarrier that
+// nothing completes; throws the engine's "device wait timed out" error when
+// the kernel recorded it (the bounded-wait path of the row transforms).
+void device_wait_check(uint32_t polls);
+
 // Smallest even / any 7-smooth integer >= n.
 int next_smooth(int n, bool even);
 
