@@ -1069,12 +1069,12 @@ template <typename T> class EngineImpl final : public Engine {
         cudaFree(dpost);
         return best;
     }
-    template <int... R> void tune_row_ct(CtRadices<R...>, size_t smem) { set_smem(k_row_r2c_ct<256, 2, R...>, smem); }
+    template <int... R> void tune_row_ct(CtRadices<R...>, size_t smem) { set_smem(k_row_r2c_ct<CT_ROW_NT, 2, R...>, smem); }
     template <int... R>
     void launch_tune_row_ct(CtRadices<R...>, const cx<T> *post, const T *plane, const cx<T> *tw, const CUtensorMap &map,
                             size_t smem) {
         dim3 grid((unsigned)ceil_div(H_, 2), 1);
-        k_row_r2c_ct<256, 2, R...><<<grid, 256, smem, stream_>>>(reinterpret_cast<const cx<float> *>(post),
+        k_row_r2c_ct<CT_ROW_NT, 2, R...><<<grid, CT_ROW_NT, smem, stream_>>>(reinterpret_cast<const cx<float> *>(post),
                                                                  reinterpret_cast<const float *>(plane), W_, H_, 0,
                                                                  reinterpret_cast<const cx<float> *>(tw), map);
     }
@@ -1456,9 +1456,9 @@ template <typename T> class EngineImpl final : public Engine {
     }
     size_t ct_row_smem() const { return row_tma_smem(2, M_, sizeof(cx<float>), 31); }
     template <int... R> void configure_rows_ct(CtRadices<R...>) {
-        set_smem(k_gather_row_r2c_ct<256, R...>, ct_row_smem());
-        set_smem(k_row_r2c_ct<256, 2, R...>, ct_row_smem());
-        set_smem(k_row_c2r_ct<256, 2, R...>, ct_row_smem());
+        set_smem(k_gather_row_r2c_ct<CT_ROW_NT, R...>, ct_row_smem());
+        set_smem(k_row_r2c_ct<CT_ROW_NT, 2, R...>, ct_row_smem());
+        set_smem(k_row_c2r_ct<CT_ROW_NT, 2, R...>, ct_row_smem());
     }
     template <int... R> void configure_cols_ct(CtRadices<R...>) {
         const size_t b = (size_t)FH_ * sizeof(cx<float>);
@@ -1470,7 +1470,7 @@ template <typename T> class EngineImpl final : public Engine {
     template <int... R>
     void launch_row_r2c_ct(CtRadices<R...>, const float *plane, int batch, size_t plane_stride, const CUtensorMap &map) {
         dim3 grid((unsigned)ceil_div(H_, 2), (unsigned)batch);
-        k_row_r2c_ct<256, 2, R...><<<grid, 256, ct_row_smem(), stream_>>>(
+        k_row_r2c_ct<CT_ROW_NT, 2, R...><<<grid, CT_ROW_NT, ct_row_smem(), stream_>>>(
             reinterpret_cast<const cx<float> *>(post_), plane, W_, H_, plane_stride,
             reinterpret_cast<const cx<float> *>(ct_tw_row_), map);
         UPDC_CUDA(cudaGetLastError());
@@ -1479,7 +1479,7 @@ template <typename T> class EngineImpl final : public Engine {
     // R2C (compile-time row transforms only): the scatter plane is not written.
     template <int... R> void launch_gather_row_r2c_ct(CtRadices<R...>) {
         dim3 grid((unsigned)ceil_div(H_, 2), (unsigned)act_n_);
-        k_gather_row_r2c_ct<256, R...><<<grid, 256, ct_row_smem(), stream_>>>(
+        k_gather_row_r2c_ct<CT_ROW_NT, R...><<<grid, CT_ROW_NT, ct_row_smem(), stream_>>>(
             reinterpret_cast<const cx<float> *>(post_), reinterpret_cast<const ExpDesc<float> *>(d_exps_ + act_k0_),
             reinterpret_cast<const float *>(wr_ + (size_t)act_k0_ * nin_), nin_, W_, H_,
             reinterpret_cast<const cx<float> *>(ct_tw_row_), map_rs_);
@@ -1491,7 +1491,7 @@ template <typename T> class EngineImpl final : public Engine {
     }
     template <int... R> void launch_row_c2r_ct(CtRadices<R...>, int batch, float *out, const CUtensorMap &map) {
         dim3 grid((unsigned)ceil_div(H_, 2), (unsigned)batch);
-        k_row_c2r_ct<256, 2, R...><<<grid, 256, ct_row_smem(), stream_>>>(
+        k_row_c2r_ct<CT_ROW_NT, 2, R...><<<grid, CT_ROW_NT, ct_row_smem(), stream_>>>(
             reinterpret_cast<const cx<float> *>(post_), map, H_, W_, (float)scale_factor(), out, nout_,
             reinterpret_cast<const cx<float> *>(ct_tw_row_), d_err_);
         UPDC_CUDA(cudaGetLastError());
@@ -1843,7 +1843,7 @@ template <typename T> class EngineImpl final : public Engine {
             const DevLinkMap &m = links_[k];
             ExpDesc<T> &d = h[k];
             d.off = m.off; d.base = m.base; d.tgt = m.tgt; d.delta = m.delta; d.frac = m.frac;
-            d.toff = m.toff; d.tsrc = m.tsrc; d.tfrac = m.tfrac;
+            d.toff = m.toff; d.tent = m.tent;
             d.sci = sci_ + (size_t)k * nin_;
             d.wht = wht_ + (size_t)k * nin_;
             d.frozen = frozen_ + (size_t)k * nin_;

@@ -26,6 +26,19 @@
 
 namespace updc {
 
+// Threads and resident blocks per SM of the compile-time row kernels, and
+// resident blocks per SM of the column kernels.
+#ifndef UPDC_CT_ROW_NT
+#define UPDC_CT_ROW_NT 256
+#endif
+#ifndef UPDC_CT_ROW_MINB
+#define UPDC_CT_ROW_MINB 4
+#endif
+#ifndef UPDC_CT_COL_MINB
+#define UPDC_CT_COL_MINB 3
+#endif
+constexpr int CT_ROW_NT = UPDC_CT_ROW_NT;
+
 // A compile-time radix list (the catalog's entries).
 template <int... R> struct CtRadices {
     static constexpr int n = CtProd<R...>::value;
@@ -66,7 +79,7 @@ struct RowPairIn {
 };
 
 template <int NT, int BR, int... R>
-__global__ void __launch_bounds__(NT, 4)
+__global__ void __launch_bounds__(NT, UPDC_CT_ROW_MINB)
     k_row_r2c_ct(const cx<float> *__restrict__ post, const float *__restrict__ planes, int W, int rows,
                  size_t plane_stride, const cx<float> *__restrict__ tw, const __grid_constant__ CUtensorMap omap) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -100,8 +113,9 @@ __device__ __forceinline__ void gather_chains(const ExpDesc<float> &e, const flo
 #pragma unroll
             for (int i = 0; i < CH; ++i) {
                 const bool ok = i0[g] + i < b[g];
-                sr[g][i] = ok ? e.tsrc[i0[g] + i] : 0u;
-                fr[g][i] = ok ? e.tfrac[i0[g] + i] : 0.f;
+                const uint2 en = ok ? e.tent[i0[g] + i] : make_uint2(0u, 0u);
+                sr[g][i] = en.x;
+                fr[g][i] = __uint_as_float(en.y);
             }
 #pragma unroll
         for (int g = 0; g < G; ++g)
@@ -135,7 +149,7 @@ __device__ __forceinline__ void gather_chains(const ExpDesc<float> &e, const flo
 // stay coalesced) and loads the next step's CSR offsets before walking this
 // step's entries.
 template <int NT, int... R>
-__global__ void __launch_bounds__(NT, 4)
+__global__ void __launch_bounds__(NT, UPDC_CT_ROW_MINB)
     k_gather_row_r2c_ct(const cx<float> *__restrict__ post, const ExpDesc<float> *__restrict__ exps,
                         const float *__restrict__ wr_all, size_t nin, int W, int rows,
                         const cx<float> *__restrict__ tw, const __grid_constant__ CUtensorMap omap) {
@@ -210,7 +224,7 @@ struct RowPairOut {
 };
 
 template <int NT, int BR, int... R>
-__global__ void __launch_bounds__(NT, 4)
+__global__ void __launch_bounds__(NT, UPDC_CT_ROW_MINB)
     k_row_c2r_ct(const cx<float> *__restrict__ post, const __grid_constant__ CUtensorMap imap, int rows, int W,
                  float scale, float *__restrict__ planes, size_t plane_stride, const cx<float> *__restrict__ tw,
                  unsigned long long *__restrict__ err) {
@@ -321,7 +335,7 @@ struct ColForwardOut {
 };
 
 template <int NT, int... R>
-__global__ void __launch_bounds__(NT, 3)
+__global__ void __launch_bounds__(NT, UPDC_CT_COL_MINB)
     k_col_forward_ct(const cx<float> *__restrict__ rx, int ldr, int rows_in, const cx<float> *__restrict__ khat,
                      size_t khat_stride, int nexp, cx<float> *__restrict__ y, int ldy, size_t y_stride, int rows_out,
                      cx<float> *__restrict__ aux, const cx<float> *__restrict__ tw) {
@@ -368,7 +382,7 @@ struct ColIn {
 };
 
 template <class Acc, int NT, int... R>
-__global__ void __launch_bounds__(NT, 3)
+__global__ void __launch_bounds__(NT, UPDC_CT_COL_MINB)
     k_col_adjoint_ct(const cx<float> *__restrict__ rs, int ldr, size_t rs_stride, int rows_in,
                      const cx<float> *__restrict__ khat, size_t khat_stride, int nexp, cx<float> *__restrict__ c,
                      int ldc, int rows_out, typename Acc::S *__restrict__ aux, const cx<float> *__restrict__ tw) {

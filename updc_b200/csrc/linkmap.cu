@@ -14,12 +14,12 @@
 namespace updc {
 
 void DevLinkMap::release() {
-    for (void *p : {(void *)off, (void *)base, (void *)tgt, (void *)delta, (void *)frac, (void *)toff, (void *)tsrc,
-                    (void *)tfrac})
+    for (void *p : {(void *)off, (void *)base, (void *)tgt, (void *)delta, (void *)frac, (void *)toff, (void *)tent})
         if (p) cudaFree(p);
-    off = base = tgt = toff = tsrc = nullptr;
+    off = base = tgt = toff = nullptr;
+    tent = nullptr;
     delta = nullptr;
-    frac = tfrac = nullptr;
+    frac = nullptr;
 }
 
 size_t linkmap_expected_bytes(const LinkMapHeader &h, size_t nin) {
@@ -328,32 +328,27 @@ __global__ void k_fill_u32(uint32_t *p, uint32_t v, size_t n) {
 
 __global__ void k_lm_scatter_entries(const uint32_t *__restrict__ owner, const uint32_t *__restrict__ target,
                                      const float *__restrict__ frac, uint64_t nlinks, const uint32_t *__restrict__ toff,
-                                     uint32_t *__restrict__ cursor, uint32_t *__restrict__ tsrc, float *__restrict__ tfrac) {
+                                     uint32_t *__restrict__ cursor, uint2 *__restrict__ tent) {
     for (size_t z = blockIdx.x * (size_t)blockDim.x + threadIdx.x; z < nlinks; z += (size_t)gridDim.x * blockDim.x) {
         const uint32_t t = target[z];
         if (t == 0xFFFFFFFFu) continue;
         const uint32_t pos = toff[t] + atomicAdd(&cursor[t], 1u);
-        tsrc[pos] = owner[z];
-        tfrac[pos] = frac[z];
+        tent[pos] = make_uint2(owner[z], __float_as_uint(frac[z]));
     }
 }
 
 // insertion sort of each target's short segment by source pixel
-__global__ void k_lm_sort_segments(const uint32_t *__restrict__ toff, size_t nout, uint32_t *__restrict__ tsrc,
-                                   float *__restrict__ tfrac) {
+__global__ void k_lm_sort_segments(const uint32_t *__restrict__ toff, size_t nout, uint2 *__restrict__ tent) {
     for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nout; t += (size_t)gridDim.x * blockDim.x) {
         const uint32_t a = toff[t], b = toff[t + 1];
         for (uint32_t i = a + 1; i < b; ++i) {
-            const uint32_t ks = tsrc[i];
-            const float kf = tfrac[i];
+            const uint2 k = tent[i];
             uint32_t j = i;
-            while (j > a && tsrc[j - 1] > ks) {
-                tsrc[j] = tsrc[j - 1];
-                tfrac[j] = tfrac[j - 1];
+            while (j > a && tent[j - 1].x > k.x) {
+                tent[j] = tent[j - 1];
                 --j;
             }
-            tsrc[j] = ks;
-            tfrac[j] = kf;
+            tent[j] = k;
         }
     }
 }
@@ -396,10 +391,9 @@ void linkmap_transpose(DevLinkMap &m, size_t nout, cudaStream_t s) {
     void *tmp = dev_alloc<char>(tmp_bytes);
     cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, cnt, m.toff, (int)(nout + 1), s);
     UPDC_CUDA(cudaMemsetAsync(cnt, 0, (nout + 1) * 4, s));
-    m.tsrc = dev_alloc<uint32_t>(nl);
-    m.tfrac = dev_alloc<float>(nl);
-    k_lm_scatter_entries<<<grid_for(nl, 256), 256, 0, s>>>(owner, target, m.frac, nl, m.toff, cnt, m.tsrc, m.tfrac);
-    k_lm_sort_segments<<<grid_for(nout, 256), 256, 0, s>>>(m.toff, nout, m.tsrc, m.tfrac);
+    m.tent = dev_alloc<uint2>(nl);
+    k_lm_scatter_entries<<<grid_for(nl, 256), 256, 0, s>>>(owner, target, m.frac, nl, m.toff, cnt, m.tent);
+    k_lm_sort_segments<<<grid_for(nout, 256), 256, 0, s>>>(m.toff, nout, m.tent);
     UPDC_CUDA(cudaGetLastError());
     UPDC_CUDA(cudaStreamSynchronize(s));
     cudaFree(owner);

@@ -36,11 +36,12 @@ struct DevLinkMap {
     uint32_t *off = nullptr, *base = nullptr, *tgt = nullptr;
     uint16_t *delta = nullptr;
     float *frac = nullptr;
-    // transpose: for target t, entries [toff[t], toff[t+1]) hold (source pixel,
-    // fraction) in increasing source-pixel order, the order in which the
-    // reference's serial scatter loop visits them.
-    uint32_t *toff = nullptr, *tsrc = nullptr;
-    float *tfrac = nullptr;
+    // transpose: for target t, entries [toff[t], toff[t+1]) hold {source
+    // pixel, fraction bits} (one 8-byte entry each) in increasing
+    // source-pixel order, the order in which the reference's serial scatter
+    // loop visits them.
+    uint32_t *toff = nullptr;
+    uint2 *tent = nullptr;
     void release();
 };
 

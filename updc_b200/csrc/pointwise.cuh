@@ -10,8 +10,8 @@ template <typename T> struct ExpDesc {
     const uint32_t *off, *base, *tgt;
     const uint16_t *delta;
     const float *frac;
-    const uint32_t *toff, *tsrc;
-    const float *tfrac;
+    const uint32_t *toff;
+    const uint2 *tent;  // transposed entries {source pixel, fraction bits}
     const T *sci, *wht;
     uint8_t *frozen;
     T background, pedestal, mean_offset;
@@ -337,8 +337,9 @@ __device__ __forceinline__ void scatter_targets(const ExpDesc<T> &e, size_t nout
 #pragma unroll
             for (int i = 0; i < CH; ++i) {
                 const bool ok = ic + i < b;
-                src[i] = ok ? e.tsrc[ic + i] : 0u;
-                fr[i] = ok ? e.tfrac[ic + i] : 0.0f;
+                const uint2 en = ok ? e.tent[ic + i] : make_uint2(0u, 0u);
+                src[i] = en.x;
+                fr[i] = __uint_as_float(en.y);
             }
 #pragma unroll
             for (int i = 0; i < CH; ++i) {
@@ -667,10 +668,11 @@ __global__ void __launch_bounds__(256) k_drizzle(const ExpDesc<T> *__restrict__ 
             const ExpDesc<T> &e = exps[k];
             const uint32_t a = e.toff[t], b = e.toff[t + 1];
             for (uint32_t i = a; i < b; ++i) {
-                const uint32_t p = e.tsrc[i];
+                const uint2 en = e.tent[i];
+                const uint32_t p = en.x;
                 const T w = e.wht[p];
                 if (!(w > T(0))) continue;
-                const T q = mul_rn((T)e.tfrac[i], w);
+                const T q = mul_rn((T)__uint_as_float(en.y), w);
                 cov = add_rn(cov, q);
                 data = fma_rn(q, e.sci[p], data);
                 bkg = fma_rn(q, e.background, bkg);
