@@ -175,6 +175,48 @@ def test_large_column_transforms(engine_lib, oracle, datasets, form, tol):
     assert rel_rms(e2.plane("estimate", as_double=True), s64.estimate) <= 10 * tol
 
 
+@pytest.mark.parametrize("form,tol", [("fp32", 2e-6), ("fp64", 1e-12)])
+def test_long_row_transforms(engine_lib, oracle, datasets, form, tol):
+    """FFT widths whose rows exceed one block (FW/2 = 6000 > 5632 complex
+    points) take the four-step long-row kernels (6000 = 10 x 600): forward
+    model, denominator and two iterations against the FP64 oracle on the same
+    shape."""
+    ds = datasets("c0")
+    shape = (12000, 288)
+    e = _engine(ds, form=form, fft_shape=shape)
+    assert e.fft_shape == shape
+    s64 = _oracle_solver(oracle, ds, precision=64, fft_shape=shape)
+    assert rel_rms(e.plane("denominator", as_double=True), s64.denominator) <= tol
+    e.set_plane("estimate", s64.estimate)
+    e.stage_forward()
+    for k in range(ds.workload.nexp):
+        assert rel_rms(e.plane("blur", k, as_double=True), s64.forward_blur(k)) <= tol
+    e2 = _engine(ds, form=form, fft_shape=shape)
+    e2.iterate(2)
+    s64.iterate(2)
+    assert rel_rms(e2.plane("estimate", as_double=True), s64.estimate) <= 10 * tol
+    e.close()
+    e2.close()
+
+
+def test_wide_abs32_field_matches_reference_core(engine_lib, reference_binary, datasets, tmp_path):
+    """The reference's ABS32 validation geometry (a 66000-pixel-wide target,
+    docs/V17_VALIDATION.md): ABS32 LinkMaps built on the GPU, rows of
+    33075 complex points through the four-step kernels; the whole solve within
+    1e-5 relative RMS of the reference core, with the same FreezeMu counts."""
+    ds = datasets("abs32_wide")
+    w = ds.workload
+    xref, rows = _reference_run(reference_binary, ds, w.iterations, tmp_path)
+    e = _engine(ds, form="fp32")
+    assert e.fft_shape[0] // 2 > 5632
+    assert all(e.link_encoding(k) == 1 for k in range(w.nexp))
+    st = e.iterate(w.iterations)
+    assert rel_rms(e.plane("estimate"), xref) <= 1e-5
+    assert [(int(s.new_frozen[k]), int(s.total_frozen[k])) for s in st for k in range(w.nexp)] == \
+        [(int(r["n_new_frozen"]), int(r["n_total_frozen"])) for r in rows]
+    e.close()
+
+
 @pytest.mark.parametrize("shape", [(3600, 300), (3840, 288)])
 @pytest.mark.parametrize("form,tol", [("fp32", 2e-6), ("fp64", 1e-12)])
 def test_two_row_tiles(engine_lib, oracle, datasets, form, tol, shape):

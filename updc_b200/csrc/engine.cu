@@ -14,6 +14,7 @@
 #include "fft.cuh"
 #include "kernels.cuh"
 #include "kernels_ct.cuh"
+#include "longrow.cuh"
 #include "linkmap.cuh"
 #include "pointwise.cuh"
 #include "nll.cuh"
@@ -623,6 +624,7 @@ template <typename T> class EngineImpl final : public Engine {
 
     FieldView field_view() const override {
         if (!setup_done_) throw Error(1, "engine is not set up");
+        if (long_rows_) throw Error(1, "batched fields need FFT widths within the row-transform capacity");
         FieldView v;
         v.elem_bytes = sizeof(T);
         v.form = opt_.form;
@@ -732,6 +734,13 @@ template <typename T> class EngineImpl final : public Engine {
         UPDC_CUDA(cudaMemsetAsync(d_psf_grad_, 0, count * 8, stream_));
         const int fwid = transposed_ ? e.psf_height : e.psf_width, fhei = transposed_ ? e.psf_width : e.psf_height;
         const PsfWindowStore<T> epi{d_psf_grad_, e.psf_width, fwid, fhei, FW_, FH_, transposed_};
+        if (long_rows_) {
+            long_c2r<T>(lrp_, post_, SpecRef{xs, FH_, 0}, FH_, 1, FW_, (T)(1.0 / ((double)FW_ * (double)FH_)), epi,
+                        long_scratch_);
+            UPDC_CUDA(cudaMemcpyAsync(out, d_psf_grad_, count * 8, cudaMemcpyDeviceToHost, stream_));
+            UPDC_CUDA(cudaStreamSynchronize(stream_));
+            return;
+        }
         const int B = row_b_;
         const size_t rsm = row_buf_bytes(B, M_, sizeof(cx<T>), plan_m_.pad_shift);
         set_smem(k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PsfWindowStore<T>, false>, rsm);
@@ -811,7 +820,7 @@ template <typename T> class EngineImpl final : public Engine {
             case 8: return choice_.candidates;
             case 9: return choice_.cache_hit ? 1 : 0;
             case 10: return choice_.predicted_ms;
-            case 11: return (ct_rows() ? 1 : 0) | (ct_cols() ? 2 : 0) | (fused_gather() ? 4 : 0);
+            case 11: return (ct_rows() ? 1 : 0) | (ct_cols() ? 2 : 0) | (fused_gather() ? 4 : 0) | (long_rows_ ? 8 : 0);
             default: return 0;
         }
     }
@@ -1235,7 +1244,11 @@ template <typename T> class EngineImpl final : public Engine {
         if ((opt_.fft_width && (opt_.fft_width < min_w || (opt_.fft_width & 1))) || (opt_.fft_height && opt_.fft_height < min_h))
             throw Error(1, "FFT shape below the minimum length or odd width");
         FftChoice c;
-        if (opt_.autotune) {
+        // rows longer than one block holds (FW/2 above the row capacity) take
+        // the four-step long-row kernels at the smallest width; the
+        // autotuner times single-block row splits only
+        const bool long_min = min_w / 2 > Caps<T>::ROW || (opt_.fft_width && opt_.fft_width / 2 > Caps<T>::ROW);
+        if (opt_.autotune && !long_min) {
             const std::string cache = tune_cache_path(min_w, min_h);
             const double t0 = now_s();
             if (load_tune_cache(cache, min_w, min_h, c) && (!opt_.fft_width || c.width == opt_.fft_width) &&
@@ -1254,7 +1267,9 @@ template <typename T> class EngineImpl final : public Engine {
         FW_ = c.width;
         FH_ = c.height;
         M_ = FW_ / 2;
-        if (M_ > Caps<T>::ROW) throw Error(1, "FFT width exceeds the row-transform capacity");
+        long_rows_ = M_ > Caps<T>::ROW;
+        if (long_rows_ && !long_row_split(M_, Caps<T>::ROW, lrp_.M1, lrp_.M2))
+            throw Error(1, "FFT width exceeds the row-transform capacity");
         if (FH_ > Caps<T>::COL_L) throw Error(1, "FFT height exceeds the column-transform capacity");
         // a catalog split (compile-time kernels) is preferred where the length
         // has one and nothing was tuned; a split that is neither a catalog
@@ -1314,6 +1329,62 @@ template <typename T> class EngineImpl final : public Engine {
         for (int u = 0; u <= M_; ++u) post[u] = cx<T>{(T)std::cos(-two_pi * u / FW_), (T)std::sin(-two_pi * u / FW_)};
         post_ = alloc<cx<T>>(M_ + 1);
         UPDC_CUDA(cudaMemcpy(post_, post.data(), post.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
+        if (long_rows_) lrp_ = make_long_plan<T>(lrp_.M1, lrp_.M2, [&](size_t n) { return (void *)alloc<cx<T>>(n); });
+    }
+
+    // ------------------------------------------------------------------ long rows (longrow.cuh)
+    bool long_rows_ = false;
+    LongRowPlan lrp_;
+    cx<T> *long_scratch_ = nullptr;  // planes x rows x M of the long-row passes
+    // Plans and tables of precision U for M = M1 * M2; `get(n)` allocates n
+    // complex values of U on the device.
+    template <typename U, class Get> LongRowPlan make_long_plan(int M1, int M2, Get &&get) {
+        LongRowPlan lp;
+        lp.M1 = M1, lp.M2 = M2, lp.M = M1 * M2;
+        auto t1 = fft_make_table<U>(M1, FFT_RMAX, lp.p1);
+        auto t2 = fft_make_table<U>(M2, FFT_RMAX, lp.p2);
+        lp.p1.pad_shift = lp.p2.pad_shift = 31;
+        std::vector<cx<U>> tm(lp.M);
+        const double two_pi = 6.283185307179586476925286766559;
+        for (int e = 0; e < lp.M; ++e) tm[e] = cx<U>{(U)std::cos(-two_pi * e / lp.M), (U)std::sin(-two_pi * e / lp.M)};
+        cx<U> *d1 = (cx<U> *)get(t1.size()), *d2 = (cx<U> *)get(t2.size()), *dm = (cx<U> *)get(tm.size());
+        UPDC_CUDA(cudaMemcpy(d1, t1.data(), t1.size() * sizeof(cx<U>), cudaMemcpyHostToDevice));
+        UPDC_CUDA(cudaMemcpy(d2, t2.data(), t2.size() * sizeof(cx<U>), cudaMemcpyHostToDevice));
+        UPDC_CUDA(cudaMemcpy(dm, tm.data(), tm.size() * sizeof(cx<U>), cudaMemcpyHostToDevice));
+        lp.p1.tw = d1;
+        lp.p2.tw = d2;
+        lp.twm = dm;
+        return lp;
+    }
+    // Real rows [0, rows) of `planes` planes (through the loader) -> u-major
+    // bins in `out`, four-step; `scratch` holds planes x rows x M.
+    template <typename U, class Loader>
+    void long_r2c(const LongRowPlan &lp, const Loader &ld, int W, int rows, int planes, const cx<U> *post, SpecRef out,
+                  cx<U> *scratch) {
+        constexpr int NT = RowNt<U>::value, CAP = Caps<U>::ROW;
+        const size_t sa = (size_t)LONG_G * lp.M2 * sizeof(cx<U>), sb = 2 * (size_t)lp.M1 * sizeof(cx<U>);
+        set_smem(k_long_r2c_a<U, NT, CAP, Loader>, sa);
+        set_smem(k_long_r2c_b<U, NT, CAP>, sb);
+        k_long_r2c_a<U, NT, CAP, Loader><<<dim3((unsigned)ceil_div(lp.M1, LONG_G), rows, planes), NT, sa, stream_>>>(
+            lp, ld, W, rows, scratch);
+        k_long_r2c_b<U, NT, CAP><<<dim3((unsigned)(lp.M2 / 2 + 1), rows, planes), NT, sb, stream_>>>(lp, scratch, post,
+                                                                                                   rows, out);
+        UPDC_CUDA(cudaGetLastError());
+    }
+    // u-major bins `in` of `planes` planes -> cropped, scaled real rows through
+    // the epilogue, four-step.
+    template <typename U, class Epi>
+    void long_c2r(const LongRowPlan &lp, const cx<U> *post, SpecRef in, int rows, int planes, int W, U scale,
+                  const Epi &epi, cx<U> *scratch) {
+        constexpr int NT = RowNt<U>::value, CAP = Caps<U>::ROW;
+        const size_t sa = 2 * (size_t)lp.M1 * sizeof(cx<U>), sb = (size_t)LONG_G * lp.M2 * sizeof(cx<U>);
+        set_smem(k_long_c2r_a<U, NT, CAP>, sa);
+        set_smem(k_long_c2r_b<U, NT, CAP, Epi>, sb);
+        k_long_c2r_a<U, NT, CAP><<<dim3((unsigned)ceil_div(lp.M2, 2), rows, planes), NT, sa, stream_>>>(lp, post, in, rows,
+                                                                                                      scratch);
+        k_long_c2r_b<U, NT, CAP, Epi><<<dim3((unsigned)ceil_div(lp.M1, LONG_G), rows, planes), NT, sb, stream_>>>(
+            lp, scratch, rows, W, scale, epi);
+        UPDC_CUDA(cudaGetLastError());
     }
 
     void allocate() {
@@ -1363,7 +1434,9 @@ template <typename T> class EngineImpl final : public Engine {
         // the FFT buffer and the staging tile share the block's shared memory
         while (row_b_ > 2 && row_tma_smem(row_b_, M_, sizeof(cx<T>), plan_m_.pad_shift) > SMEM_LIMIT)
             row_b_ -= EW == 1 ? 2 : 1;
-        use_tma_ = (row_b_ * EW) % 2 == 0 && row_tma_smem(row_b_, M_, sizeof(cx<T>), plan_m_.pad_shift) <= SMEM_LIMIT;
+        use_tma_ = !long_rows_ && (row_b_ * EW) % 2 == 0 &&
+                   row_tma_smem(row_b_, M_, sizeof(cx<T>), plan_m_.pad_shift) <= SMEM_LIMIT;
+        if (long_rows_) long_scratch_ = alloc<cx<T>>((size_t)std::max(nexp_ * H_, FH_) * M_);
         if (!ct_row_rad_.empty() && !(use_tma_ && row_b_ == 2)) {
             // the compile-time row kernels take two-row TMA tiles
             ct_row_rad_.clear();
@@ -1418,16 +1491,26 @@ template <typename T> class EngineImpl final : public Engine {
     }
 
     void configure_kernels() {
-        const size_t rs = row_smem();
-        by_pad(plan_m_.pad_shift, [&](auto P) {
-            by_rows(row_b_, [&](auto Q) {
-                constexpr int PS = decltype(P)::value, BR = decltype(Q)::value;
-                set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, true, PS, BR>, rs);
-                set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false, PS, BR>, rs);
-                set_smem(k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, true, PS, BR>, rs);
-                set_smem(k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, false, PS, BR>, rs);
+        if (long_rows_) {
+            // the iteration's long-row launches (attributes set before any capture)
+            constexpr int NT = RowNt<T>::value, CAP = Caps<T>::ROW;
+            const size_t sg = (size_t)LONG_G * lrp_.M2 * sizeof(cx<T>), s2 = 2 * (size_t)lrp_.M1 * sizeof(cx<T>);
+            set_smem(k_long_r2c_a<T, NT, CAP, PlaneLoader<T>>, sg);
+            set_smem(k_long_r2c_b<T, NT, CAP>, s2);
+            set_smem(k_long_c2r_a<T, NT, CAP>, s2);
+            set_smem(k_long_c2r_b<T, NT, CAP, PlaneStore<T>>, sg);
+        } else {
+            const size_t rs = row_smem();
+            by_pad(plan_m_.pad_shift, [&](auto P) {
+                by_rows(row_b_, [&](auto Q) {
+                    constexpr int PS = decltype(P)::value, BR = decltype(Q)::value;
+                    set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, true, PS, BR>, rs);
+                    set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, false, PS, BR>, rs);
+                    set_smem(k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, true, PS, BR>, rs);
+                    set_smem(k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PlaneStore<T>, false, PS, BR>, rs);
+                });
             });
-        });
+        }
         const size_t fs = fwd_smem();
         by_pad(plan_h_.pad_shift, [&](auto P) {
             constexpr int PS = decltype(P)::value;
@@ -1512,6 +1595,11 @@ template <typename T> class EngineImpl final : public Engine {
     // ------------------------------------------------------------------ launches
     // planes [batch][H][W] -> u-major spectra [batch][M+1][ldh], one launch
     void launch_row_r2c_plane(const T *plane, cx<T> *out, int batch, size_t plane_stride, const CUtensorMap &map) {
+        if (long_rows_) {
+            long_r2c<T>(lrp_, PlaneLoader<T>{plane, W_, plane_stride}, W_, H_, batch, post_,
+                        SpecRef{out, ldh_, (size_t)(M_ + 1) * ldh_}, long_scratch_);
+            return;
+        }
         if constexpr (sizeof(T) == 4) {
             if (ct_rows()) {
                 ct_row_catalog(ct_row_rad_, [&](auto L) { launch_row_r2c_ct(L, plane, batch, plane_stride, map); });
@@ -1605,6 +1693,11 @@ template <typename T> class EngineImpl final : public Engine {
         launch_col_adjoint_t<AccPlain<T>>(khat_);
     }
     void launch_row_c2r_batched(const cx<T> *in, int batch, T *out, const CUtensorMap &map) {
+        if (long_rows_) {
+            long_c2r<T>(lrp_, post_, SpecRef{const_cast<cx<T> *>(in), ldh_, (size_t)(M_ + 1) * ldh_}, H_, batch, W_,
+                        scale_factor(), PlaneStore<T>{out, W_, nout_}, long_scratch_);
+            return;
+        }
         if constexpr (sizeof(T) == 4) {
             if (ct_rows()) {
                 ct_row_catalog(ct_row_rad_, [&](auto L) { launch_row_c2r_ct(L, batch, out, map); });
@@ -1976,21 +2069,34 @@ template <typename T> class EngineImpl final : public Engine {
             if (fp64_sum) inv = (U)(1.0 / sum);
             else inv = (U)(1.0f / (float)sum);
             PsfLoader<U, P> ld{dp, pw, transposed_ ? phh : pw, transposed_ ? pw : phh, FW_, FH_, transposed_, inv};
+            if (long_rows_) {
+                // four-step rows; a temporary plan and scratch of precision U
+                std::vector<void *> owned;
+                auto get = [&](size_t n) {
+                    owned.push_back(dalloc<cx<U>>(n, nullptr));
+                    return owned.back();
+                };
+                try {
+                    const LongRowPlan lp = make_long_plan<U>(lrp_.M1, lrp_.M2, get);
+                    cx<U> *scr = (cx<U> *)get((size_t)FH_ * M_);
+                    long_r2c<U>(lp, ld, FW_, FH_, 1, post, SpecRef{rp, FH_, 0}, scr);
+                    col_fft_psf<U>(ph, rp, out);
+                    UPDC_CUDA(cudaStreamSynchronize(stream_));
+                } catch (...) {
+                    for (void *q : owned) cudaFree(q);
+                    throw;
+                }
+                for (void *q : owned) cudaFree(q);
+                cudaFree(dp);
+                return;
+            }
             const int B = Caps<U>::ROW / M_;
             const size_t rsm = row_buf_bytes(B, M_, sizeof(cx<U>), pm.pad_shift);
             set_smem(k_row_r2c<U, RowNt<U>::value, Caps<U>::ROW, PsfLoader<U, P>, false>, rsm);
             dim3 grid((unsigned)ceil_div(FH_, B), 1);
             k_row_r2c<U, RowNt<U>::value, Caps<U>::ROW, PsfLoader<U, P>, false><<<grid, RowNt<U>::value, rsm, stream_>>>(
                 pm, post, ld, FW_, FH_, B, FastDiv((uint32_t)B), SpecRef{rp, FH_, 0}, no_map_);
-            const size_t cs = fft_buf_bytes(FH_, sizeof(cx<U>), ph.pad_shift);
-            if (FH_ <= Caps<U>::COL_S) {
-                set_smem(k_col_fft<U, NT, Caps<U>::COL_S, false>, cs);
-                k_col_fft<U, NT, Caps<U>::COL_S, false><<<(unsigned)nu, NT, cs, stream_>>>(ph, rp, FH_, FH_, out, FH_, FH_);
-            } else {
-                set_smem(k_col_fft<U, NT, Caps<U>::COL_L, false>, cs);
-                k_col_fft<U, NT, Caps<U>::COL_L, false><<<(unsigned)nu, NT, cs, stream_>>>(ph, rp, FH_, FH_, out, FH_, FH_);
-            }
-            UPDC_CUDA(cudaGetLastError());
+            col_fft_psf<U>(ph, rp, out);
             UPDC_CUDA(cudaStreamSynchronize(stream_));
         } catch (...) {
             cudaFree(dp);
@@ -2025,6 +2131,20 @@ template <typename T> class EngineImpl final : public Engine {
         finish_denominator();
     }
 
+    // Column FFTs of the PSF's row-pass output rp ((M+1) x FH) into out.
+    template <typename U> void col_fft_psf(const FftPlan &ph, const cx<U> *rp, cx<U> *out) {
+        const size_t nu = (size_t)M_ + 1;
+        const size_t cs = fft_buf_bytes(FH_, sizeof(cx<U>), ph.pad_shift);
+        if (FH_ <= Caps<U>::COL_S) {
+            set_smem(k_col_fft<U, NT, Caps<U>::COL_S, false>, cs);
+            k_col_fft<U, NT, Caps<U>::COL_S, false><<<(unsigned)nu, NT, cs, stream_>>>(ph, rp, FH_, FH_, out, FH_, FH_);
+        } else {
+            set_smem(k_col_fft<U, NT, Caps<U>::COL_L, false>, cs);
+            k_col_fft<U, NT, Caps<U>::COL_L, false><<<(unsigned)nu, NT, cs, stream_>>>(ph, rp, FH_, FH_, out, FH_, FH_);
+        }
+        UPDC_CUDA(cudaGetLastError());
+    }
+
     // FP32 form: the one-time denominator is computed entirely in FP64.
     void denominator_fp64() {
         using D = double;
@@ -2050,10 +2170,22 @@ template <typename T> class EngineImpl final : public Engine {
         dim3 grid((unsigned)std::min<size_t>(ceil_div(nout_, 256), 148 * 8), (unsigned)nexp_);
         k_scatter_t<T, D, T><<<grid, 256, 0, stream_>>>(d_exps_, nin_, nout_, (const T *)nullptr, 1, sc);
         cx<D> *rs = dalloc<cx<D>>(nexp_ * nu * H_, nullptr), *cr = dalloc<cx<D>>(nu * H_, nullptr);
-        const int B = Caps<D>::ROW / M_;
+        const int B = std::max(1, Caps<D>::ROW / M_);
         const size_t rsm = row_buf_bytes(B, M_, sizeof(cx<D>), pm.pad_shift);
-        set_smem(k_row_r2c<D, RowNt<D>::value, Caps<D>::ROW, PlaneLoader<D>, false>, rsm);
-        {
+        // long rows: an FP64 four-step plan and its scratch, freed below
+        std::vector<void *> lowned;
+        LongRowPlan lpd;
+        cx<D> *lscr = nullptr;
+        if (long_rows_) {
+            auto get = [&](size_t n) {
+                lowned.push_back(dalloc<cx<D>>(n, nullptr));
+                return lowned.back();
+            };
+            lpd = make_long_plan<D>(lrp_.M1, lrp_.M2, get);
+            lscr = (cx<D> *)get((size_t)nexp_ * H_ * M_);
+            long_r2c<D>(lpd, PlaneLoader<D>{sc, W_, nout_}, W_, H_, nexp_, dpost, SpecRef{rs, H_, nu * H_}, lscr);
+        } else {
+            set_smem(k_row_r2c<D, RowNt<D>::value, Caps<D>::ROW, PlaneLoader<D>, false>, rsm);
             dim3 g((unsigned)ceil_div(H_, B), (unsigned)nexp_);
             k_row_r2c<D, RowNt<D>::value, Caps<D>::ROW, PlaneLoader<D>, false><<<g, RowNt<D>::value, rsm, stream_>>>(
                 pm, dpost, PlaneLoader<D>{sc, W_, nout_}, W_, H_, B, FastDiv((uint32_t)B), SpecRef{rs, H_, nu * H_}, no_map_);
@@ -2070,16 +2202,22 @@ template <typename T> class EngineImpl final : public Engine {
             k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_L><<<(unsigned)nu, NtAdj<D>::value, s, stream_>>>(ph, rs, H_, nu * H_, H_, kd, nu * FH_, nexp_, cr, H_, H_, aux);
         }
         D *den = dalloc<D>(nout_, nullptr);
-        set_smem(k_row_c2r<D, RowNt<D>::value, Caps<D>::ROW, PlaneStore<D>, false>, rsm);
-        dim3 g2((unsigned)ceil_div(H_, B), 1);
-        k_row_c2r<D, RowNt<D>::value, Caps<D>::ROW, PlaneStore<D>, false><<<g2, RowNt<D>::value, rsm, stream_>>>(
-            pm, dpost, SpecRef{cr, H_, 0}, no_map_, H_, W_, B, FastDiv((uint32_t)B), 1.0 / (double)((size_t)FW_ * FH_),
-            PlaneStore<D>{den, W_, 0}, d_err_);
+        if (long_rows_) {
+            long_c2r<D>(lpd, dpost, SpecRef{cr, H_, 0}, H_, 1, W_, 1.0 / (double)((size_t)FW_ * FH_),
+                        PlaneStore<D>{den, W_, 0}, lscr);
+        } else {
+            set_smem(k_row_c2r<D, RowNt<D>::value, Caps<D>::ROW, PlaneStore<D>, false>, rsm);
+            dim3 g2((unsigned)ceil_div(H_, B), 1);
+            k_row_c2r<D, RowNt<D>::value, Caps<D>::ROW, PlaneStore<D>, false><<<g2, RowNt<D>::value, rsm, stream_>>>(
+                pm, dpost, SpecRef{cr, H_, 0}, no_map_, H_, W_, B, FastDiv((uint32_t)B), 1.0 / (double)((size_t)FW_ * FH_),
+                PlaneStore<D>{den, W_, 0}, d_err_);
+        }
         k_convert<D, T><<<grid1d(nout_), 256, 0, stream_>>>(den, den_, nout_);
         UPDC_CUDA(cudaGetLastError());
         UPDC_CUDA(cudaStreamSynchronize(stream_));
         for (void *p : {(void *)dm, (void *)dh, (void *)dpost, (void *)kd, (void *)sc, (void *)rs, (void *)cr, (void *)aux, (void *)den})
             if (p) cudaFree(p);
+        for (void *p : lowned) cudaFree(p);
     }
 
     void finish_denominator() {

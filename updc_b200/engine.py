@@ -182,10 +182,12 @@ class Engine:
     @property
     def kernel_variants(self) -> dict:
         """Which specialised kernels the iteration runs: row / column transforms
-        compiled for their radix sequence, and the adjoint gather fused into
-        the scatter row transform (no scatter plane)."""
+        compiled for their radix sequence, the adjoint gather fused into the
+        scatter row transform (no scatter plane), and four-step rows for FFT
+        widths beyond one block."""
         v = int(self.scalar(11))
-        return {"compiled_rows": bool(v & 1), "compiled_columns": bool(v & 2), "fused_gather": bool(v & 4)}
+        return {"compiled_rows": bool(v & 1), "compiled_columns": bool(v & 2), "fused_gather": bool(v & 4),
+                "long_rows": bool(v & 8)}
 
     @property
     def masked_pixels(self) -> int:

@@ -80,7 +80,7 @@ WORKLOADS: Dict[str, Workload] = {
     "abs32": Workload("abs32", 3400, 48, 6, 2, 2, 3, "gauss_moffat", 3, 0, 2,
                       scale=20.0, dither_max=0.5, seed=5),
     # the reference's own ABS32 validation geometry (target width 70000 class);
-    # CPU oracle only: its rows exceed the GPU row-transform capacity
+    # (rows of 33075 complex points: the GPU engine's four-step long-row path)
     "abs32_wide": Workload("abs32_wide", 66000, 6, 6, 2, 2, 3, "gauss_moffat", 3, 0, 2,
                            scale=2.0, dither_max=0.5, seed=5),
 }
