@@ -563,7 +563,8 @@ def preprocess_arm(args, rank, world, local_rank):
 
 def sharded_arm(args, rank, world, local_rank):
     """N > 1: one field, its exposures split over the ranks (contiguous
-    shares), every rank set up on the whole field; per iteration each rank
+    shares), every rank set up on its own share (the setup's cross-exposure
+    sums all-reduced once); per iteration each rank
     computes the partial correction of its exposures, one NCCL all-reduce
     sums them, and every rank applies the same update.  Total work is fixed
     (strong scaling); time is the max over ranks of the device-timed loop."""
@@ -581,7 +582,7 @@ def sharded_arm(args, rank, world, local_rank):
         ds = synth.generate(w.name, workdir, use_torch=True)
         t0 = time.time()
         shard = open_engine_shard(str(ds.manifest), w.W, w.H, w.iw, w.ih, w.nexp, rank, world, form=args.form,
-                                  device=local_rank)
+                                  device=local_rank, dist=dist)
         solver = ShardedSolver(shard, dist)
         setup_s = time.time() - t0
         solver.iterate(args.warmup)

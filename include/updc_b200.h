@@ -187,6 +187,17 @@ int updc_copy_plane_device(updc_engine *h, int which, int exposure, void *device
  * after the DENOMINATOR plane was replaced. */
 int updc_set_active_exposures(updc_engine *h, int first, int count);
 int updc_refresh_sensitivity(updc_engine *h);
+/* Shard setup (no reference counterpart): updc_set_active_exposures called
+ * between updc_load_manifest and updc_setup sets the shard up alone — only
+ * its exposures' LinkMaps and PSF spectra are built — and updc_setup leaves
+ * partial planes: COVERAGE, ESTIMATE (the drizzle's data sum), CORRECTION
+ * (its background sum) and DENOMINATOR, each over the shard's exposures.  The
+ * caller sums each of the four over the shards in place (e.g. NCCL
+ * all-reduce through updc_plane_device_pointer) and calls
+ * updc_finish_shard_setup, which forms the drizzle estimate and the maximum
+ * sensitivity; iterations are refused until then.  Results equal the whole
+ * field's up to the order of the cross-shard sums. */
+int updc_finish_shard_setup(updc_engine *h);
 /* The same exchange without host round trips (no reference counterpart):
  * updc_plane_device_pointer gives the engine's own device address of a
  * target plane (ESTIMATE, COVERAGE, DENOMINATOR or CORRECTION: W x H

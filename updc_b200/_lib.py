@@ -103,6 +103,7 @@ def load() -> ctypes.CDLL:
     L.updc_set_active_exposures.argtypes = [P, c.c_int, c.c_int]
     L.updc_refresh_sensitivity.argtypes = [P]
     L.updc_device_wait_check.argtypes = [c.c_uint32]
+    L.updc_finish_shard_setup.argtypes = [P]
     L.updc_plane_device_pointer.argtypes = [P, c.c_int, c.POINTER(c.c_void_p)]
     L.updc_engine_stream.argtypes = [P, c.POINTER(c.c_void_p)]
     L.updc_enqueue_partial.argtypes = [P]

@@ -273,6 +273,12 @@ int updc_refresh_sensitivity(updc_engine *h) {
         h->e->refresh_sensitivity();
     });
 }
+int updc_finish_shard_setup(updc_engine *h) {
+    return guarded([&] {
+        if (!h) throw Error(1, "null handle");
+        h->e->finish_shard_setup();
+    });
+}
 int updc_plane_device_pointer(updc_engine *h, int which, void **device_ptr) {
     return guarded([&] {
         if (!h || !device_ptr) throw Error(1, "null handle or output pointer");

@@ -354,7 +354,8 @@ template <typename T> class EngineImpl final : public Engine {
         choose_fft_shape();
         allocate();
         double t0 = now_s();
-        for (int k = 0; k < nexp_; ++k) prepare_links(k);
+        for (int k = 0; k < nexp_; ++k)
+            if (active(k)) prepare_links(k);
         setup_time_[0] = now_s() - t0;
         t0 = now_s();
         load_planes();
@@ -369,7 +370,10 @@ template <typename T> class EngineImpl final : public Engine {
         denominator();
         setup_time_[4] = now_s() - t0;
         setup_time_[5] = now_s() - t_all;
-        setup_done_ = true;
+        // an exposure shard set up alone waits for its partial planes to be
+        // summed over the shards (finish_shard_setup)
+        setup_done_ = !shard_setup_;
+        shard_setup_pending_ = shard_setup_;
     }
 
     void iterate(int n, bool check_each, std::vector<IterationRecord> *records) override {
@@ -554,8 +558,15 @@ template <typename T> class EngineImpl final : public Engine {
         make_tensor_map_3d(&map_rs_, act_rs(), d0, (uint64_t)M_ + 1, act_n_, row_b_ * EW, ub);
     }
     void set_active_exposures(int k0, int n) override {
-        if (!setup_done_) throw Error(1, "engine is not set up");
         if (k0 < 0 || n < 1 || k0 + n > nexp_) throw Error(1, "active exposure range out of bounds");
+        if (!setup_done_) {
+            // before setup: set up this exposure shard alone (see setup)
+            if (shard_setup_pending_) throw Error(1, "shard setup is waiting for finish_shard_setup");
+            act_k0_ = k0;
+            act_n_ = n;
+            shard_setup_ = n < nexp_;
+            return;
+        }
         act_k0_ = k0;
         act_n_ = n;
         build_exposure_maps();
@@ -566,6 +577,24 @@ template <typename T> class EngineImpl final : public Engine {
         graph_ = nullptr;
     }
     void refresh_sensitivity() override { finish_denominator(); }
+    // Shard setup: only exposures [act_k0_, act_k0_ + act_n_) get LinkMaps
+    // and PSF spectra, and the drizzle and denominator leave partial planes
+    // (COVERAGE, ESTIMATE = the data sum, CORRECTION = the background sum,
+    // DENOMINATOR) for the caller to sum over the shards.
+    bool shard_setup_ = false, shard_setup_pending_ = false;
+    bool active(int k) const { return !shard_setup_ || (k >= act_k0_ && k < act_k0_ + act_n_); }
+    void finish_shard_setup() override {
+        if (!shard_setup_pending_) throw Error(1, "no shard setup is waiting for its sums");
+        UPDC_CUDA(cudaMemset(d_err_, 0xFF, 8));
+        k_drizzle_finish<T><<<grid1d(nout_), 256, 0, stream_>>>(nout_, coverage_, estimate_, correction_, estimate_, d_err_);
+        UPDC_CUDA(cudaGetLastError());
+        UPDC_CUDA(cudaMemsetAsync(correction_, 0, nout_ * sizeof(T), stream_));
+        UPDC_CUDA(cudaStreamSynchronize(stream_));
+        check_error();
+        finish_denominator();
+        shard_setup_pending_ = false;
+        setup_done_ = true;
+    }
 
     // ------------------------------------------------------------------ checkpoint / resume
     // State file: a 64-byte header {"UPDCSTAT", u32 version 1, u32 element
@@ -1448,8 +1477,10 @@ template <typename T> class EngineImpl final : public Engine {
             make_tensor_map_3d(&map_rx_, rx_, d0, nu, 1, row_b_ * EW, ub);
             make_tensor_map_3d(&map_cr_, cr_, d0, nu, 1, row_b_ * EW, ub);
         }
-        act_k0_ = 0;
-        act_n_ = nexp_;
+        if (!shard_setup_) {
+            act_k0_ = 0;
+            act_n_ = nexp_;
+        }
         build_exposure_maps();
         configure_kernels();
         // the adjoint's accumulator plane, when it does not fit shared memory,
@@ -2016,6 +2047,7 @@ template <typename T> class EngineImpl final : public Engine {
         cx<U> *rp = dalloc<cx<U>>(nu * FH_, nullptr);
         try {
             for (int k = 0; k < nexp_; ++k) {
+                if (!active(k)) continue;
                 const ExposureInput &e = exps_[k];
                 const size_t count = (size_t)e.psf_width * e.psf_height;
                 std::vector<float> hp(count);
@@ -2111,6 +2143,13 @@ template <typename T> class EngineImpl final : public Engine {
     }
 
     void drizzle() {
+        if (shard_setup_) {
+            k_drizzle_partial<T><<<grid1d(nout_), 256, 0, stream_>>>(d_exps_ + act_k0_, act_n_, nout_, coverage_, estimate_,
+                                                                    correction_);
+            UPDC_CUDA(cudaGetLastError());
+            UPDC_CUDA(cudaStreamSynchronize(stream_));
+            return;
+        }
         UPDC_CUDA(cudaMemset(d_err_, 0xFF, 8));
         k_drizzle<T><<<grid1d(nout_), 256, 0, stream_>>>(d_exps_, nexp_, nout_, estimate_, coverage_, d_err_);
         UPDC_CUDA(cudaGetLastError());
@@ -2120,15 +2159,18 @@ template <typename T> class EngineImpl final : public Engine {
 
     // D = crop(C2R(sum_k conj(K_k) R2C(pad(S_k^T W_k)))) / nf   (updc_core.c:1026-1086)
     void denominator() {
+        // the active exposures' terms (all of them unless this is a shard set up alone)
         if (sizeof(T) == 4 && opt_.form == FORM_FP32) denominator_fp64();
         else {
-            dim3 grid((unsigned)std::min<size_t>(ceil_div(nout_, 256), 148 * 8), (unsigned)nexp_);
-            k_scatter_t<T, T, T><<<grid, 256, 0, stream_>>>(d_exps_, nin_, nout_, (const T *)nullptr, 1, scatter_);
-            launch_row_r2c_plane(scatter_, rs_, nexp_, nout_, map_rs_);
+            dim3 grid((unsigned)std::min<size_t>(ceil_div(nout_, 256), 148 * 8), (unsigned)act_n_);
+            k_scatter_t<T, T, T><<<grid, 256, 0, stream_>>>(d_exps_ + act_k0_, nin_, nout_, (const T *)nullptr, 1,
+                                                            scatter_ + (size_t)act_k0_ * nout_);
+            launch_row_r2c_plane(scatter_ + (size_t)act_k0_ * nout_, act_rs(), act_n_, nout_, map_rs_);
             launch_col_adjoint();
             launch_row_c2r_batched(cr_, 1, den_, map_cr_);
         }
-        finish_denominator();
+        if (shard_setup_) UPDC_CUDA(cudaStreamSynchronize(stream_));
+        else finish_denominator();
     }
 
     // Column FFTs of the PSF's row-pass output rp ((M+1) x FH) into out.
@@ -2167,8 +2209,9 @@ template <typename T> class EngineImpl final : public Engine {
         cx<D> *kd = dalloc<cx<D>>(nexp_ * nu * FH_, nullptr);
         psf_spectra<D>(kd, true, pm, ph, dpost);
         D *sc = dalloc<D>(nexp_ * nout_, nullptr);
-        dim3 grid((unsigned)std::min<size_t>(ceil_div(nout_, 256), 148 * 8), (unsigned)nexp_);
-        k_scatter_t<T, D, T><<<grid, 256, 0, stream_>>>(d_exps_, nin_, nout_, (const T *)nullptr, 1, sc);
+        // the active exposures' terms (all of them unless this is a shard set up alone)
+        dim3 grid((unsigned)std::min<size_t>(ceil_div(nout_, 256), 148 * 8), (unsigned)act_n_);
+        k_scatter_t<T, D, T><<<grid, 256, 0, stream_>>>(d_exps_ + act_k0_, nin_, nout_, (const T *)nullptr, 1, sc);
         cx<D> *rs = dalloc<cx<D>>(nexp_ * nu * H_, nullptr), *cr = dalloc<cx<D>>(nu * H_, nullptr);
         const int B = std::max(1, Caps<D>::ROW / M_);
         const size_t rsm = row_buf_bytes(B, M_, sizeof(cx<D>), pm.pad_shift);
@@ -2183,10 +2226,10 @@ template <typename T> class EngineImpl final : public Engine {
             };
             lpd = make_long_plan<D>(lrp_.M1, lrp_.M2, get);
             lscr = (cx<D> *)get((size_t)nexp_ * H_ * M_);
-            long_r2c<D>(lpd, PlaneLoader<D>{sc, W_, nout_}, W_, H_, nexp_, dpost, SpecRef{rs, H_, nu * H_}, lscr);
+            long_r2c<D>(lpd, PlaneLoader<D>{sc, W_, nout_}, W_, H_, act_n_, dpost, SpecRef{rs, H_, nu * H_}, lscr);
         } else {
             set_smem(k_row_r2c<D, RowNt<D>::value, Caps<D>::ROW, PlaneLoader<D>, false>, rsm);
-            dim3 g((unsigned)ceil_div(H_, B), (unsigned)nexp_);
+            dim3 g((unsigned)ceil_div(H_, B), (unsigned)act_n_);
             k_row_r2c<D, RowNt<D>::value, Caps<D>::ROW, PlaneLoader<D>, false><<<g, RowNt<D>::value, rsm, stream_>>>(
                 pm, dpost, PlaneLoader<D>{sc, W_, nout_}, W_, H_, B, FastDiv((uint32_t)B), SpecRef{rs, H_, nu * H_}, no_map_);
         }
@@ -2196,10 +2239,10 @@ template <typename T> class EngineImpl final : public Engine {
         const size_t s = aux_needed ? b : b + align16(FH_ * sizeof(cx<D>));
         if (FH_ <= Caps<D>::COL_S) {
             set_smem(k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_S>, s);
-            k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_S><<<(unsigned)nu, NtAdj<D>::value, s, stream_>>>(ph, rs, H_, nu * H_, H_, kd, nu * FH_, nexp_, cr, H_, H_, aux);
+            k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_S><<<(unsigned)nu, NtAdj<D>::value, s, stream_>>>(ph, rs, H_, nu * H_, H_, kd + (size_t)act_k0_ * nu * FH_, nu * FH_, act_n_, cr, H_, H_, aux);
         } else {
             set_smem(k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_L>, s);
-            k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_L><<<(unsigned)nu, NtAdj<D>::value, s, stream_>>>(ph, rs, H_, nu * H_, H_, kd, nu * FH_, nexp_, cr, H_, H_, aux);
+            k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_L><<<(unsigned)nu, NtAdj<D>::value, s, stream_>>>(ph, rs, H_, nu * H_, H_, kd + (size_t)act_k0_ * nu * FH_, nu * FH_, act_n_, cr, H_, H_, aux);
         }
         D *den = dalloc<D>(nout_, nullptr);
         if (long_rows_) {

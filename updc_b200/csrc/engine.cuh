@@ -115,7 +115,13 @@ class Engine {
     virtual void copy_plane_device(int which, int k, void *dptr, int to_engine, int as_double, cudaStream_t stream) = 0;
     // Iterate only exposures [k0, k0 + n) (an exposure shard of a multi-GPU
     // solve: every other setup product stays that of the whole field).
+    // Called before setup(), the shard is set up alone: LinkMaps and PSF
+    // spectra of its exposures only, and the drizzle and denominator leave
+    // partial planes (COVERAGE, ESTIMATE = data sum, CORRECTION = background
+    // sum, DENOMINATOR) that the caller sums over the shards before
+    // finish_shard_setup() forms the estimate and the maximum sensitivity.
     virtual void set_active_exposures(int k0, int n) = 0;
+    virtual void finish_shard_setup() = 0;
     // Recompute max_sensitivity from the denominator plane (after it was
     // replaced, e.g. by a sum over shards).
     virtual void refresh_sensitivity() = 0;

@@ -688,6 +688,50 @@ __global__ void __launch_bounds__(256) k_drizzle(const ExpDesc<T> *__restrict__ 
     }
 }
 
+// The drizzle's three per-target sums over exposures [0, nexp) of `exps`
+// only (an exposure shard, set up alone): coverage, data and background, in
+// the order k_drizzle forms them.  The shards' planes are summed over ranks,
+// then k_drizzle_finish forms the estimate as k_drizzle does.
+template <typename T>
+__global__ void __launch_bounds__(256) k_drizzle_partial(const ExpDesc<T> *__restrict__ exps, int nexp, size_t nout,
+                                                         T *__restrict__ coverage, T *__restrict__ data,
+                                                         T *__restrict__ background) {
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nout; t += (size_t)gridDim.x * blockDim.x) {
+        T cov = 0, dat = 0, bkg = 0;
+        for (int k = 0; k < nexp; ++k) {
+            const ExpDesc<T> &e = exps[k];
+            const uint32_t a = e.toff[t], b = e.toff[t + 1];
+            for (uint32_t i = a; i < b; ++i) {
+                const uint2 en = e.tent[i];
+                const uint32_t p = en.x;
+                const T w = e.wht[p];
+                if (!(w > T(0))) continue;
+                const T q = mul_rn((T)__uint_as_float(en.y), w);
+                cov = add_rn(cov, q);
+                dat = fma_rn(q, e.sci[p], dat);
+                bkg = fma_rn(q, e.background, bkg);
+            }
+        }
+        coverage[t] = cov;
+        data[t] = dat;
+        background[t] = bkg;
+    }
+}
+template <typename T>
+__global__ void __launch_bounds__(256) k_drizzle_finish(size_t nout, const T *__restrict__ coverage,
+                                                        const T *__restrict__ data, const T *__restrict__ background,
+                                                        T *__restrict__ estimate, unsigned long long *__restrict__ err) {
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nout; t += (size_t)gridDim.x * blockDim.x) {
+        const T cov = coverage[t];
+        T est = T(0);
+        if (cov > (T)1e-12f) {
+            est = sub_rn(div_rn(data[t], cov), div_rn(background[t], cov));
+            if (!isfinite(est)) record_error(err, STAGE_SETUP, t, ERR_NONFINITE_INITIAL);
+        }
+        estimate[t] = est;
+    }
+}
+
 template <typename A, typename B>
 __global__ void k_convert(const A *__restrict__ in, B *__restrict__ out, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) out[i] = (B)in[i];

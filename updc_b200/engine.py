@@ -238,6 +238,12 @@ class Engine:
     def refresh_sensitivity(self) -> None:
         check(self._L.updc_refresh_sensitivity(self._h))
 
+    def finish_shard_setup(self) -> None:
+        """After a shard setup (set_active_exposures before setup) and the sum
+        of its partial planes over the shards: the drizzle estimate and the
+        maximum sensitivity."""
+        check(self._L.updc_finish_shard_setup(self._h))
+
     def plane_device_pointer(self, name: str) -> int:
         """The engine's own device address of a target plane (W x H elements
         of the form's precision), valid until close()."""

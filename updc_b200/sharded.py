@@ -2,10 +2,11 @@
 
 The iteration of updc/c_core/updc_core.c:1410-1456 sums the adjoint of every
 exposure before its single inverse transform (core:1280-1287); that sum is
-the only place exposures meet.  So each rank sets up the whole field
-(LinkMaps, PSF spectra, the drizzle x0 and the denominator D over all
-exposures, identical on every rank) and then iterates only its own
-contiguous share of the exposures: forward model, detector loop, transposed
+the only place exposures meet.  So each rank sets up only its own
+contiguous share of the exposures (LinkMaps, PSF spectra), the setup's
+cross-exposure sums (the drizzle x0's coverage, data and background, and the
+denominator D) are all-reduced once, and every rank then iterates its
+share: forward model, detector loop, transposed
 gather and adjoint of its exposures give a partial correction plane, the
 partial planes are summed over ranks with one all-reduce, and every rank
 applies the same multiplicative update, so the estimate stays replicated
@@ -160,10 +161,30 @@ class ShardedSolver:
 
 
 def open_engine_shard(manifest: str, W: int, H: int, iw: int, ih: int, nexp: int, rank: int, world: int,
-                      form: str = "fp32", device: int = 0, **engine_kw) -> EngineShard:
-    """Set up the whole field on this rank's GPU and keep its exposure shard."""
+                      form: str = "fp32", device: int = 0, dist=None, group=None, **engine_kw) -> EngineShard:
+    """This rank's exposure shard on its GPU.  With `dist` and more than one
+    rank the shard is set up alone — LinkMaps and PSF spectra of its own
+    exposures only — and the partial planes the setup leaves (coverage, the
+    drizzle's data and background sums, the denominator) are all-reduced
+    before the engine finishes the drizzle estimate and the maximum
+    sensitivity; results then equal the whole field's up to the order of the
+    cross-rank sums.  Without, every rank sets up the whole field."""
+    import torch
     from .engine import Engine
     e = Engine(form=form, device=device, use_graph=False, **engine_kw)
-    e.load(manifest, W, H, iw, ih, nexp).setup()
+    e.load(manifest, W, H, iw, ih, nexp)
     first, count = shard_range(nexp, rank, world)
+    if dist is not None and world > 1:
+        e.set_active_exposures(first, count)
+        e.setup()
+        dev = torch.cuda.current_device()
+        stream = torch.cuda.ExternalStream(e.stream_handle(), device=dev)
+        with torch.cuda.stream(stream):
+            for name in ("coverage", "estimate", "correction", "denominator"):
+                plane = torch.as_tensor(_DevicePlane(e.plane_device_pointer(name), (H, W), form == "fp64"), device=dev)
+                dist.all_reduce(plane, op=dist.ReduceOp.SUM, group=group)
+        stream.synchronize()
+        e.finish_shard_setup()
+    else:
+        e.setup()
     return EngineShard(e, first, count)
