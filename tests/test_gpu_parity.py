@@ -175,14 +175,16 @@ def test_large_column_transforms(engine_lib, oracle, datasets, form, tol):
     assert rel_rms(e2.plane("estimate", as_double=True), s64.estimate) <= 10 * tol
 
 
+@pytest.mark.parametrize("shape", [(12000, 288), (288, 12000)])
 @pytest.mark.parametrize("form,tol", [("fp32", 2e-6), ("fp64", 1e-12)])
-def test_long_row_transforms(engine_lib, oracle, datasets, form, tol):
-    """FFT widths whose rows exceed one block (FW/2 = 6000 > 5632 complex
-    points) take the four-step long-row kernels (6000 = 10 x 600): forward
+def test_long_row_transforms(engine_lib, oracle, datasets, form, tol, shape):
+    """FFT shapes beyond one block's transform: rows of FW/2 = 6000 > 5632
+    complex points (four-step rows, 6000 = 10 x 600) and columns of
+    FH = 12000 > 11264 points (four-step columns, 12000 = 10 x 1200, with the
+    OTF product and the cross-exposure sum as separate passes): forward
     model, denominator and two iterations against the FP64 oracle on the same
     shape."""
     ds = datasets("c0")
-    shape = (12000, 288)
     e = _engine(ds, form=form, fft_shape=shape)
     assert e.fft_shape == shape
     s64 = _oracle_solver(oracle, ds, precision=64, fft_shape=shape)

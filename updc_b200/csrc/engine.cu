@@ -653,7 +653,7 @@ template <typename T> class EngineImpl final : public Engine {
 
     FieldView field_view() const override {
         if (!setup_done_) throw Error(1, "engine is not set up");
-        if (long_rows_) throw Error(1, "batched fields need FFT widths within the row-transform capacity");
+        if (long_rows_ || long_cols_) throw Error(1, "batched fields need FFT shapes within the one-block transform capacity");
         FieldView v;
         v.elem_bytes = sizeof(T);
         v.form = opt_.form;
@@ -815,6 +815,7 @@ template <typename T> class EngineImpl final : public Engine {
     // column transforms of M+1 columns: `in` has `rows_in` rows at pitch ldi
     template <bool INV> void launch_col_fft(const cx<T> *in, int ldi, int rows_in, cx<T> *out, int ldo, int rows_out) {
         const size_t nu = (size_t)M_ + 1;
+        if (long_cols_) return long_col_fft<T, INV>(lcp_, in, ldi, rows_in, out, ldo, rows_out, (int)nu, long_col_scratch_);
         const size_t cs = fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift);
         if (FH_ <= Caps<T>::COL_S) {
             set_smem(k_col_fft<T, NT, Caps<T>::COL_S, INV>, cs);
@@ -1276,7 +1277,8 @@ template <typename T> class EngineImpl final : public Engine {
         // rows longer than one block holds (FW/2 above the row capacity) take
         // the four-step long-row kernels at the smallest width; the
         // autotuner times single-block row splits only
-        const bool long_min = min_w / 2 > Caps<T>::ROW || (opt_.fft_width && opt_.fft_width / 2 > Caps<T>::ROW);
+        const bool long_min = min_w / 2 > Caps<T>::ROW || (opt_.fft_width && opt_.fft_width / 2 > Caps<T>::ROW) ||
+                              min_h > Caps<T>::COL_L || opt_.fft_height > Caps<T>::COL_L;
         if (opt_.autotune && !long_min) {
             const std::string cache = tune_cache_path(min_w, min_h);
             const double t0 = now_s();
@@ -1299,7 +1301,9 @@ template <typename T> class EngineImpl final : public Engine {
         long_rows_ = M_ > Caps<T>::ROW;
         if (long_rows_ && !long_row_split(M_, Caps<T>::ROW, lrp_.M1, lrp_.M2))
             throw Error(1, "FFT width exceeds the row-transform capacity");
-        if (FH_ > Caps<T>::COL_L) throw Error(1, "FFT height exceeds the column-transform capacity");
+        long_cols_ = FH_ > Caps<T>::COL_L;
+        if (long_cols_ && !long_col_split(FH_, Caps<T>::COL_L, lcp_.N1, lcp_.N2))
+            throw Error(1, "FFT height exceeds the column-transform capacity");
         // a catalog split (compile-time kernels) is preferred where the length
         // has one and nothing was tuned; a split that is neither a catalog
         // entry nor a valid run-time one (non-increasing radices <= 16, e.g.
@@ -1347,7 +1351,7 @@ template <typename T> class EngineImpl final : public Engine {
             (axis ? ct_tw_col_ : ct_tw_row_) = d;
         }
         plan_m_.pad_shift = fft_choose_padding(plan_m_, RowNt<T>::value, Caps<T>::ROW, std::max(1, std::min(2, Caps<T>::ROW / M_)));
-        plan_h_.pad_shift = fft_choose_padding(plan_h_, ColNt<T>::value, Caps<T>::COL_S, 1);
+        plan_h_.pad_shift = long_cols_ ? 31 : fft_choose_padding(plan_h_, ColNt<T>::value, Caps<T>::COL_S, 1);
         cx<T> *dm = alloc<cx<T>>(tm.size()), *dh = alloc<cx<T>>(th.size());
         UPDC_CUDA(cudaMemcpy(dm, tm.data(), tm.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
         UPDC_CUDA(cudaMemcpy(dh, th.data(), th.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
@@ -1359,6 +1363,69 @@ template <typename T> class EngineImpl final : public Engine {
         post_ = alloc<cx<T>>(M_ + 1);
         UPDC_CUDA(cudaMemcpy(post_, post.data(), post.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
         if (long_rows_) lrp_ = make_long_plan<T>(lrp_.M1, lrp_.M2, [&](size_t n) { return (void *)alloc<cx<T>>(n); });
+        if (long_cols_) lcp_ = col_plan(make_long_plan<T>(lcp_.N1, lcp_.N2, [&](size_t n) { return (void *)alloc<cx<T>>(n); }));
+    }
+
+    // ------------------------------------------------------------------ long columns (longrow.cuh)
+    bool long_cols_ = false;
+    LongColPlan lcp_;
+    cx<T> *long_col_scratch_ = nullptr, *long_col_tmp_ = nullptr;  // (M+1) x FH each
+    static LongColPlan col_plan(const LongRowPlan &r) {
+        LongColPlan c;
+        c.N = r.M, c.N1 = r.M1, c.N2 = r.M2, c.p1 = r.p1, c.p2 = r.p2, c.twm = r.twm;
+        return c;
+    }
+    // Column FFTs (forward, or unnormalised inverse) of length FH of `ncols`
+    // u-rows, four-step: rows [0, rows_in) of each input column (zero beyond)
+    // to rows [0, rows_out) of the output.
+    template <typename U, bool INV>
+    void long_col_fft(const LongColPlan &lp, const cx<U> *in, int ld_in, int rows_in, cx<U> *out, int ld_out,
+                      int rows_out, int ncols, cx<U> *scratch) {
+        constexpr int CAP = Caps<U>::COL_L;
+        const size_t sa = (size_t)LONG_G * lp.N2 * sizeof(cx<U>), sb = (size_t)LONG_G * lp.N1 * sizeof(cx<U>);
+        set_smem(k_long_col_a<U, NT, CAP, INV>, sa);
+        set_smem(k_long_col_b<U, NT, CAP, INV>, sb);
+        k_long_col_a<U, NT, CAP, INV><<<dim3((unsigned)ceil_div(lp.N1, LONG_G), ncols), NT, sa, stream_>>>(
+            lp, in, ld_in, rows_in, scratch);
+        k_long_col_b<U, NT, CAP, INV><<<dim3((unsigned)ceil_div(lp.N2, LONG_G), ncols), NT, sb, stream_>>>(
+            lp, scratch, out, ld_out, rows_out);
+        UPDC_CUDA(cudaGetLastError());
+    }
+    void configure_long_cols() {
+        const size_t sa = (size_t)LONG_G * lcp_.N2 * sizeof(cx<T>), sb = (size_t)LONG_G * lcp_.N1 * sizeof(cx<T>);
+        constexpr int CAP = Caps<T>::COL_L;
+        set_smem(k_long_col_a<T, NT, CAP, false>, sa);
+        set_smem(k_long_col_a<T, NT, CAP, true>, sa);
+        set_smem(k_long_col_b<T, NT, CAP, false>, sb);
+        set_smem(k_long_col_b<T, NT, CAP, true>, sb);
+    }
+    // Forward model, columns: X-hat = FFT(pad(rx)), then IFFT(X-hat K_k) per
+    // active exposure into its y spectrum (unnormalised, rows < H).
+    void long_col_forward() {
+        const size_t nu = (size_t)M_ + 1, n = nu * FH_;
+        cx<T> *xh = aux_fwd_;
+        long_col_fft<T, false>(lcp_, rx_, ldh_, H_, xh, FH_, FH_, (int)nu, long_col_scratch_);
+        for (int j = 0; j < act_n_; ++j) {
+            const int k = act_k0_ + j;
+            k_long_mul<T><<<grid1d(n), 256, 0, stream_>>>(xh, khat_ + (size_t)k * n, long_col_tmp_, n);
+            long_col_fft<T, true>(lcp_, long_col_tmp_, FH_, FH_, y_ + (size_t)k * nu * ldh_, ldh_, H_, (int)nu,
+                                  long_col_scratch_);
+        }
+        UPDC_CUDA(cudaGetLastError());
+    }
+    // Adjoint, columns: the conj-OTF products of the active exposures' scatter
+    // spectra summed through the form's accumulator, then the inverse into cr.
+    template <class Acc> void long_col_adjoint(const cx<T> *khat) {
+        const size_t nu = (size_t)M_ + 1, n = nu * FH_;
+        auto *acc = (typename Acc::S *)aux_adj_;
+        for (int j = 0; j < act_n_; ++j) {
+            const int k = act_k0_ + j;
+            long_col_fft<T, false>(lcp_, rs_ + (size_t)k * nu * ldh_, ldh_, H_, long_col_tmp_, FH_, FH_, (int)nu,
+                                   long_col_scratch_);
+            k_long_acc<T, Acc><<<grid1d(n), 256, 0, stream_>>>(long_col_tmp_, khat + (size_t)k * n, acc, n, j == 0);
+        }
+        k_long_get<T, Acc><<<grid1d(n), 256, 0, stream_>>>(acc, long_col_tmp_, n);
+        long_col_fft<T, true>(lcp_, long_col_tmp_, FH_, FH_, cr_, ldh_, H_, (int)nu, long_col_scratch_);
     }
 
     // ------------------------------------------------------------------ long rows (longrow.cuh)
@@ -1452,8 +1519,13 @@ template <typename T> class EngineImpl final : public Engine {
         d_part_neg_ = alloc<unsigned long long>(upd_grid_);
         d_red_sum_ = alloc<double>(1);
         d_red_neg_ = alloc<unsigned long long>(1);
-        if (cols_in_global() || fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift) + align16((size_t)FH_ * sizeof(cx<T>)) > SMEM_LIMIT)
+        if (long_cols_ || cols_in_global() ||
+            fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift) + align16((size_t)FH_ * sizeof(cx<T>)) > SMEM_LIMIT)
             aux_fwd_ = alloc<cx<T>>(nu * FH_);
+        if (long_cols_) {
+            long_col_scratch_ = alloc<cx<T>>(nu * FH_);
+            long_col_tmp_ = alloc<cx<T>>(nu * FH_);
+        }
         links_.assign(nexp_, DevLinkMap());
         // rows per row-transform block; the TMA path needs an even number of
         // 8-byte elements per row tile (16-byte box rows and coordinates)
@@ -1542,20 +1614,24 @@ template <typename T> class EngineImpl final : public Engine {
                 });
             });
         }
-        const size_t fs = fwd_smem();
-        by_pad(plan_h_.pad_shift, [&](auto P) {
-            constexpr int PS = decltype(P)::value;
-            set_smem(k_col_forward<T, ColNt<T>::value, Caps<T>::COL_S, ColAux<T>, PS>, fs);
-            set_smem(k_col_forward<T, ColNt<T>::value, Caps<T>::COL_L, ColAux<T>, PS>, fs);
-        });
-        set_smem(k_col_fft<T, NT, Caps<T>::COL_S, false>, fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift));
-        set_smem(k_col_fft<T, NT, Caps<T>::COL_L, false>, fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift));
         set_smem(k_detector<T, true>, sizeof(DetShared));
         set_smem(k_detector<T, false>, sizeof(DetShared));
-        configure_adjoint<AccPlain<T>>();
-        if (sizeof(T) == 4) {
-            configure_adjoint<AccF64>();
-            configure_adjoint<AccKahan>();
+        if (long_cols_) {
+            configure_long_cols();
+        } else {
+            const size_t fs = fwd_smem();
+            by_pad(plan_h_.pad_shift, [&](auto P) {
+                constexpr int PS = decltype(P)::value;
+                set_smem(k_col_forward<T, ColNt<T>::value, Caps<T>::COL_S, ColAux<T>, PS>, fs);
+                set_smem(k_col_forward<T, ColNt<T>::value, Caps<T>::COL_L, ColAux<T>, PS>, fs);
+            });
+            set_smem(k_col_fft<T, NT, Caps<T>::COL_S, false>, fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift));
+            set_smem(k_col_fft<T, NT, Caps<T>::COL_L, false>, fft_buf_bytes(FH_, sizeof(cx<T>), plan_h_.pad_shift));
+            configure_adjoint<AccPlain<T>>();
+            if (sizeof(T) == 4) {
+                configure_adjoint<AccF64>();
+                configure_adjoint<AccKahan>();
+            }
         }
         if constexpr (sizeof(T) == 4) {
             if (ct_rows())
@@ -1655,6 +1731,7 @@ template <typename T> class EngineImpl final : public Engine {
         UPDC_CUDA(cudaGetLastError());
     }
     void launch_col_forward() {
+        if (long_cols_) return long_col_forward();
         const size_t nu = (size_t)M_ + 1;
         const size_t ks = nu * FH_, ys = nu * ldh_;
         if constexpr (sizeof(T) == 4) {
@@ -1717,6 +1794,13 @@ template <typename T> class EngineImpl final : public Engine {
         UPDC_CUDA(cudaGetLastError());
     }
     void launch_col_adjoint() {
+        if (long_cols_) {
+            if constexpr (sizeof(T) == 4) {
+                if (opt_.form == FORM_FP32) return long_col_adjoint<AccF64>(khat_);
+                if (opt_.form == FORM_FP32_KAHAN) return long_col_adjoint<AccKahan>(khat_);
+            }
+            return long_col_adjoint<AccPlain<T>>(khat_);
+        }
         if constexpr (sizeof(T) == 4) {
             if (opt_.form == FORM_FP32) return launch_col_adjoint_t<AccF64>(khat_);
             if (opt_.form == FORM_FP32_KAHAN) return launch_col_adjoint_t<AccKahan>(khat_);
@@ -2176,6 +2260,25 @@ template <typename T> class EngineImpl final : public Engine {
     // Column FFTs of the PSF's row-pass output rp ((M+1) x FH) into out.
     template <typename U> void col_fft_psf(const FftPlan &ph, const cx<U> *rp, cx<U> *out) {
         const size_t nu = (size_t)M_ + 1;
+        if (long_cols_) {
+            // four-step columns: a temporary plan and scratch of precision U
+            std::vector<void *> owned;
+            auto get = [&](size_t n) {
+                owned.push_back(dalloc<cx<U>>(n, nullptr));
+                return owned.back();
+            };
+            try {
+                const LongColPlan lp = col_plan(make_long_plan<U>(lcp_.N1, lcp_.N2, get));
+                cx<U> *scr = (cx<U> *)get(nu * FH_);
+                long_col_fft<U, false>(lp, rp, FH_, FH_, out, FH_, FH_, (int)nu, scr);
+                UPDC_CUDA(cudaStreamSynchronize(stream_));
+            } catch (...) {
+                for (void *q : owned) cudaFree(q);
+                throw;
+            }
+            for (void *q : owned) cudaFree(q);
+            return;
+        }
         const size_t cs = fft_buf_bytes(FH_, sizeof(cx<U>), ph.pad_shift);
         if (FH_ <= Caps<U>::COL_S) {
             set_smem(k_col_fft<U, NT, Caps<U>::COL_S, false>, cs);
@@ -2237,7 +2340,22 @@ template <typename T> class EngineImpl final : public Engine {
         const bool aux_needed = b + align16(FH_ * sizeof(cx<D>)) > SMEM_LIMIT;
         cx<D> *aux = aux_needed ? dalloc<cx<D>>(nu * FH_, nullptr) : nullptr;
         const size_t s = aux_needed ? b : b + align16(FH_ * sizeof(cx<D>));
-        if (FH_ <= Caps<D>::COL_S) {
+        if (long_cols_) {
+            // four-step FP64 columns: temporary plan, scratch, product and sum planes
+            auto get = [&](size_t n) {
+                lowned.push_back(dalloc<cx<D>>(n, nullptr));
+                return lowned.back();
+            };
+            const LongColPlan lc = col_plan(make_long_plan<D>(lcp_.N1, lcp_.N2, get));
+            const size_t n = nu * FH_;
+            cx<D> *cs = (cx<D> *)get(n), *tmp = (cx<D> *)get(n), *sum = (cx<D> *)get(n);
+            for (int j = 0; j < act_n_; ++j) {
+                long_col_fft<D, false>(lc, rs + (size_t)j * nu * H_, H_, H_, tmp, FH_, FH_, (int)nu, cs);
+                k_long_acc<D, AccPlain<D>><<<grid1d(n), 256, 0, stream_>>>(tmp, kd + (size_t)(act_k0_ + j) * n, sum, n,
+                                                                           j == 0);
+            }
+            long_col_fft<D, true>(lc, sum, FH_, FH_, cr, H_, H_, (int)nu, cs);
+        } else if (FH_ <= Caps<D>::COL_S) {
             set_smem(k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_S>, s);
             k_col_adjoint<D, AccPlain<D>, NtAdj<D>::value,Caps<D>::COL_S><<<(unsigned)nu, NtAdj<D>::value, s, stream_>>>(ph, rs, H_, nu * H_, H_, kd + (size_t)act_k0_ * nu * FH_, nu * FH_, act_n_, cr, H_, H_, aux);
         } else {

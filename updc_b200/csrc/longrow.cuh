@@ -1,4 +1,6 @@
-// Row transforms longer than one block's shared memory holds (FW/2 above the
+// Row and column transforms longer than one block's shared memory holds.
+//
+// Rows (FW/2 above the
 // row capacity of 5632 complex points): the half-length complex FFT of
 // z[m] = x[2m] + i x[2m+1] (m < M) split four-step as M = M1 * M2, both
 // factors within a block, with m = n1 + M1 n2 and bin k = k2 + M2 k1:
@@ -164,6 +166,105 @@ __global__ void __launch_bounds__(NT) k_long_c2r_b(const __grid_constant__ LongR
         if (x < W) epi(k, y, x, mul_scale(z.x, scale));
         if (x + 1 < W) epi(k, y, x + 1, mul_scale(z.y, scale));
     }
+}
+
+// ---------------------------------------------------------------------------- long columns
+// Columns longer than one block holds (FH above the column capacity): the
+// complex FFT of each u-row (column) of length N = N1 * N2, four-step with
+// n = n1 + N1 n2 and k = k2 + N2 k1, through a scratch [u][k2][n1]; inputs
+// beyond rows_in are zero, outputs past rows_out are not stored.  Pass A
+// takes LONG_G consecutive n1 of one column, pass B LONG_G consecutive k2.
+struct LongColPlan {
+    int N = 0, N1 = 0, N2 = 0;
+    FftPlan p1, p2;             // N1- and N2-point plans (no padding)
+    const void *twm = nullptr;  // cx<T>[N]: w_N^e
+};
+
+// grid (ceil(N1 / LONG_G), columns); LONG_G * N2 complex of shared memory.
+template <typename T, int NT, int CAP, bool INV>
+__global__ void __launch_bounds__(NT) k_long_col_a(const __grid_constant__ LongColPlan lp, const cx<T> *__restrict__ in,
+                                                   int ld_in, int rows_in, cx<T> *__restrict__ scratch) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
+    const int N1 = lp.N1, N2 = lp.N2;
+    const int n10 = blockIdx.x * LONG_G, u = blockIdx.y;
+    const cx<T> *src = in + (size_t)u * ld_in;
+    for (int i = threadIdx.x; i < LONG_G * N2; i += NT) {
+        const int g = i % LONG_G, n2 = i / LONG_G, n = n10 + g + N1 * n2;
+        buf[g * N2 + n2] = (n10 + g < N1 && n < rows_in) ? src[n] : cx<T>{T(0), T(0)};
+    }
+    __syncthreads();
+    fft_batch<INV, NT, CAP, FFT_RMAX, 31>(buf, LONG_G, lp.p2);
+    __syncthreads();
+    const cx<T> *twm = reinterpret_cast<const cx<T> *>(lp.twm);
+    cx<T> *dst = scratch + (size_t)u * lp.N;
+    for (int i = threadIdx.x; i < LONG_G * N2; i += NT) {
+        const int g = i % LONG_G, k2 = i / LONG_G, n1 = n10 + g;
+        if (n1 < N1) dst[(size_t)k2 * N1 + n1] = fmulc(buf[g * N2 + k2], long_twiddle<INV>(twm, lp.N, n1, k2));
+    }
+}
+
+// grid (ceil(N2 / LONG_G), columns); LONG_G * N1 complex of shared memory.
+template <typename T, int NT, int CAP, bool INV>
+__global__ void __launch_bounds__(NT) k_long_col_b(const __grid_constant__ LongColPlan lp, const cx<T> *__restrict__ scratch,
+                                                   cx<T> *__restrict__ out, int ld_out, int rows_out) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    cx<T> *buf = reinterpret_cast<cx<T> *>(smem_raw);
+    const int N1 = lp.N1, N2 = lp.N2;
+    const int k20 = blockIdx.x * LONG_G, u = blockIdx.y;
+    const cx<T> *src = scratch + (size_t)u * lp.N;
+    for (int i = threadIdx.x; i < LONG_G * N1; i += NT) {
+        const int g = i / N1, n1 = i - g * N1;
+        buf[i] = k20 + g < N2 ? src[(size_t)(k20 + g) * N1 + n1] : cx<T>{T(0), T(0)};
+    }
+    __syncthreads();
+    fft_batch<INV, NT, CAP, FFT_RMAX, 31>(buf, LONG_G, lp.p1);
+    __syncthreads();
+    cx<T> *dst = out + (size_t)u * ld_out;
+    for (int i = threadIdx.x; i < LONG_G * N1; i += NT) {
+        const int k1 = i / LONG_G, g = i - k1 * LONG_G, k2 = k20 + g;
+        const int k = k2 + N2 * k1;
+        if (k2 < N2 && k < rows_out) dst[k] = buf[g * N1 + k1];
+    }
+}
+
+// Elementwise steps of the long-column forward model and adjoint over
+// n = columns x FH values: p = a * b (the OTF product), and the conj-OTF
+// accumulation s (+)= conj(K) * v through an accumulator policy (kernels.cuh).
+template <typename T>
+__global__ void k_long_mul(const cx<T> *__restrict__ a, const cx<T> *__restrict__ b, cx<T> *__restrict__ out, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = cmul(a[i], b[i]);
+}
+template <typename T, class Acc>
+__global__ void k_long_acc(const cx<T> *__restrict__ v, const cx<T> *__restrict__ k, typename Acc::S *__restrict__ s,
+                           size_t n, int first) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        typename Acc::S a;
+        if (first) Acc::zero(a);
+        else a = s[i];
+        Acc::add(a, v[i], k[i]);
+        s[i] = a;
+    }
+}
+template <typename T, class Acc>
+__global__ void k_long_get(const typename Acc::S *__restrict__ s, cx<T> *__restrict__ out, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const auto g = Acc::get(s[i]);
+        out[i] = cx<T>{(T)g.x, (T)g.y};
+    }
+}
+
+// The factor pair of a long column length: N1 and N2 both with
+// LONG_G * N <= cap; false when there is none.
+inline bool long_col_split(int N, int cap, int &N1, int &N2) {
+    for (int d = cap / LONG_G; d >= 2; --d)
+        if (N % d == 0 && LONG_G * (N / d) <= cap) {
+            N2 = d;
+            N1 = N / d;
+            return true;
+        }
+    return false;
 }
 
 // The factor pair of a long row length: M2 the largest divisor with
