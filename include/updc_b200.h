@@ -97,7 +97,8 @@ int updc_write_plane(updc_engine *h, int which, int exposure, const void *host, 
  * ms per iteration of the tuned choice, 11 kernel variants of the iteration as
  * bits (1: row transforms compiled for their radix sequence, 2: column
  * transforms likewise, 4: adjoint gather fused into the scatter row transform,
- * 8: rows longer than one block, four-step). */
+ * 8: rows longer than one block, four-step, 16: columns likewise, 32: FP32
+ * rows of more than half a block in two-row tiles of 1024 threads). */
 double updc_scalar(updc_engine *h, int which);
 /* Radix split of an FFT axis (0: the row transform of FW/2 points, 1: the
  * column transform of FH points) in stage order; *count receives the number

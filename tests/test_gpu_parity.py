@@ -219,13 +219,15 @@ def test_wide_abs32_field_matches_reference_core(engine_lib, reference_binary, d
     e.close()
 
 
-@pytest.mark.parametrize("shape", [(3600, 300), (3840, 288)])
+@pytest.mark.parametrize("shape", [(3600, 300), (3840, 288), (9072, 288)])
 @pytest.mark.parametrize("form,tol", [("fp32", 2e-6), ("fp64", 1e-12)])
 def test_two_row_tiles(engine_lib, oracle, datasets, form, tol, shape):
     """FFT widths whose rows go two to a tile (the row kernels' two-row
     instantiation, with TMA tiles).  3600 x 300 gets unpadded row and column
-    plans (the no-padding instantiations), 3840 x 288 padded ones.  Forward
-    model and two iterations against the FP64 oracle on the same shape."""
+    plans (the no-padding instantiations), 3840 x 288 padded ones; the FP32
+    rows of 9072 x 288 (4536 complex points, more than half a block) take
+    the 1024-thread wide-row tiles.  Forward model and two iterations against
+    the FP64 oracle on the same shape."""
     ds = datasets("c0")
     e = _engine(ds, form=form, fft_shape=shape)
     assert e.fft_shape == shape

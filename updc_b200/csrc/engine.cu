@@ -658,7 +658,7 @@ template <typename T> class EngineImpl final : public Engine {
         v.elem_bytes = sizeof(T);
         v.form = opt_.form;
         v.comp_mu = comp_mu_;
-        v.W = W_, v.H = H_, v.M = M_, v.FH = FH_, v.ldh = ldh_, v.row_b = row_b_, v.nexp = nexp_;
+        v.W = W_, v.H = H_, v.M = M_, v.FH = FH_, v.ldh = ldh_, v.row_b = wide_rows_ ? 1 : row_b_, v.nexp = nexp_;
         v.upd_grid = upd_grid_;
         v.nin = nin_, v.nout = nout_;
         v.plan_m = plan_m_, v.plan_h = plan_h_;
@@ -770,7 +770,7 @@ template <typename T> class EngineImpl final : public Engine {
             UPDC_CUDA(cudaStreamSynchronize(stream_));
             return;
         }
-        const int B = row_b_;
+        const int B = wide_rows_ ? 1 : row_b_;
         const size_t rsm = row_buf_bytes(B, M_, sizeof(cx<T>), plan_m_.pad_shift);
         set_smem(k_row_c2r<T, RowNt<T>::value, Caps<T>::ROW, PsfWindowStore<T>, false>, rsm);
         dim3 grid((unsigned)ceil_div(FH_, B), 1);
@@ -850,7 +850,9 @@ template <typename T> class EngineImpl final : public Engine {
             case 8: return choice_.candidates;
             case 9: return choice_.cache_hit ? 1 : 0;
             case 10: return choice_.predicted_ms;
-            case 11: return (ct_rows() ? 1 : 0) | (ct_cols() ? 2 : 0) | (fused_gather() ? 4 : 0) | (long_rows_ ? 8 : 0);
+            case 11:
+                return (ct_rows() ? 1 : 0) | (ct_cols() ? 2 : 0) | (fused_gather() ? 4 : 0) | (long_rows_ ? 8 : 0) |
+                       (long_cols_ ? 16 : 0) | (wide_rows_ ? 32 : 0);
             default: return 0;
         }
     }
@@ -1535,6 +1537,12 @@ template <typename T> class EngineImpl final : public Engine {
         // the FFT buffer and the staging tile share the block's shared memory
         while (row_b_ > 2 && row_tma_smem(row_b_, M_, sizeof(cx<T>), plan_m_.pad_shift) > SMEM_LIMIT)
             row_b_ -= EW == 1 ? 2 : 1;
+        // FP32 rows of more than half the capacity: two-row TMA tiles in the
+        // 1024-thread "wide" instantiation (one block per SM) instead of
+        // one-row tiles with strided 8-byte accesses
+        wide_rows_ = sizeof(T) == 4 && !long_rows_ && row_b_ == 1 && M_ > Caps<T>::ROW / 2 && ldh_ >= 2 &&
+                     row_tma_smem(2, M_, sizeof(cx<T>), plan_m_.pad_shift) <= SMEM_LIMIT;
+        if (wide_rows_) row_b_ = 2;
         use_tma_ = !long_rows_ && (row_b_ * EW) % 2 == 0 &&
                    row_tma_smem(row_b_, M_, sizeof(cx<T>), plan_m_.pad_shift) <= SMEM_LIMIT;
         if (long_rows_) long_scratch_ = alloc<cx<T>>((size_t)std::max(nexp_ * H_, FH_) * M_);
@@ -1569,6 +1577,8 @@ template <typename T> class EngineImpl final : public Engine {
 
     // ------------------------------------------------------------------ kernel configuration
     int ldh_ = 0, row_b_ = 1;
+    bool wide_rows_ = false;
+    static constexpr int WIDE_NT = 1024, WIDE_CAP = 2 * Caps<T>::ROW;
     bool use_tma_ = false;
     CUtensorMap map_rx_{}, map_cr_{}, map_y_{}, map_rs_{}, no_map_{};
 
@@ -1604,7 +1614,13 @@ template <typename T> class EngineImpl final : public Engine {
             set_smem(k_long_c2r_b<T, NT, CAP, PlaneStore<T>>, sg);
         } else {
             const size_t rs = row_smem();
-            by_pad(plan_m_.pad_shift, [&](auto P) {
+            if (wide_rows_)
+                by_pad(plan_m_.pad_shift, [&](auto P) {
+                    constexpr int PS = decltype(P)::value;
+                    set_smem(k_row_r2c<T, WIDE_NT, WIDE_CAP, PlaneLoader<T>, true, PS, 2>, rs);
+                    set_smem(k_row_c2r<T, WIDE_NT, WIDE_CAP, PlaneStore<T>, true, PS, 2>, rs);
+                });
+            else by_pad(plan_m_.pad_shift, [&](auto P) {
                 by_rows(row_b_, [&](auto Q) {
                     constexpr int PS = decltype(P)::value, BR = decltype(Q)::value;
                     set_smem(k_row_r2c<T, RowNt<T>::value, Caps<T>::ROW, PlaneLoader<T>, true, PS, BR>, rs);
@@ -1717,6 +1733,17 @@ template <typename T> class EngineImpl final : public Engine {
         dim3 grid((unsigned)ceil_div(H_, B), (unsigned)batch);
         const PlaneLoader<T> ld{plane, W_, plane_stride};
         const SpecRef ref{out, ldh_, (size_t)(M_ + 1) * ldh_};
+        if constexpr (sizeof(T) == 4) {
+            if (wide_rows_) {
+                by_pad(plan_m_.pad_shift, [&](auto P) {
+                    constexpr int PS = decltype(P)::value;
+                    k_row_r2c<T, WIDE_NT, WIDE_CAP, PlaneLoader<T>, true, PS, 2><<<grid, WIDE_NT, row_smem(), stream_>>>(
+                        plan_m_, post_, ld, W_, H_, 2, FastDiv(2u), ref, map);
+                });
+                UPDC_CUDA(cudaGetLastError());
+                return;
+            }
+        }
         by_pad(plan_m_.pad_shift, [&](auto P) {
             by_rows(B, [&](auto Q) {
                 constexpr int PS = decltype(P)::value, BR = decltype(Q)::value;
@@ -1823,6 +1850,17 @@ template <typename T> class EngineImpl final : public Engine {
         dim3 grid((unsigned)ceil_div(H_, B), (unsigned)batch);
         const T scale = scale_factor();
         const SpecRef ref{const_cast<cx<T> *>(in), ldh_, (size_t)(M_ + 1) * ldh_};
+        if constexpr (sizeof(T) == 4) {
+            if (wide_rows_) {
+                by_pad(plan_m_.pad_shift, [&](auto P) {
+                    constexpr int PS = decltype(P)::value;
+                    k_row_c2r<T, WIDE_NT, WIDE_CAP, PlaneStore<T>, true, PS, 2><<<grid, WIDE_NT, row_smem(), stream_>>>(
+                        plan_m_, post_, ref, map, H_, W_, 2, FastDiv(2u), scale, PlaneStore<T>{out, W_, nout_}, d_err_);
+                });
+                UPDC_CUDA(cudaGetLastError());
+                return;
+            }
+        }
         by_pad(plan_m_.pad_shift, [&](auto P) {
             by_rows(B, [&](auto Q) {
                 constexpr int PS = decltype(P)::value, BR = decltype(Q)::value;

@@ -183,11 +183,12 @@ class Engine:
     def kernel_variants(self) -> dict:
         """Which specialised kernels the iteration runs: row / column transforms
         compiled for their radix sequence, the adjoint gather fused into the
-        scatter row transform (no scatter plane), and four-step rows for FFT
-        widths beyond one block."""
+        scatter row transform (no scatter plane), four-step rows and columns
+        for FFT shapes beyond one block, and two-row tiles of 1024 threads for
+        FP32 rows of more than half a block."""
         v = int(self.scalar(11))
         return {"compiled_rows": bool(v & 1), "compiled_columns": bool(v & 2), "fused_gather": bool(v & 4),
-                "long_rows": bool(v & 8)}
+                "long_rows": bool(v & 8), "long_columns": bool(v & 16), "wide_rows": bool(v & 32)}
 
     @property
     def masked_pixels(self) -> int:
