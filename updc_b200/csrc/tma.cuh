@@ -62,10 +62,12 @@ __device__ __forceinline__ void tma_store_3d(const CUtensorMap *map, const void 
                  : "memory");
 }
 
-// Commits the issued bulk stores and waits until they are complete.
+// Commits the issued bulk stores and waits until they have read their
+// shared-memory source (the block may then exit or reuse the tile; the
+// global writes complete with the grid, before any later kernel runs).
 __device__ __forceinline__ void tma_store_commit_and_wait() {
     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
 // Makes generic-proxy shared-memory writes visible to the TMA (async proxy).
