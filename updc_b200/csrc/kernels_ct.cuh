@@ -356,6 +356,10 @@ __global__ void __launch_bounds__(NT, UPDC_CT_ROW_MINB)
 #ifndef UPDC_CT_COL_NT
 #define UPDC_CT_COL_NT 384
 #endif
+// Accumulator and OTF elements a thread loads together in the column adjoint.
+#ifndef UPDC_COL_ADJ_B
+#define UPDC_COL_ADJ_B 4
+#endif
 constexpr int CT_COL_NT = UPDC_CT_COL_NT;
 
 // Element v = threadIdx.x + j*NT (j < ceil(N/NT)) of a column, visited in
@@ -460,7 +464,7 @@ __global__ void __launch_bounds__(NT, UPDC_CT_COL_MINB)
                      int ldc, int rows_out, typename Acc::S *__restrict__ aux, const cx<float> *__restrict__ tw) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     constexpr int N = CtProd<R...>::value;
-    constexpr int B = 4;
+    constexpr int B = UPDC_COL_ADJ_B;
     cx<float> *buf = reinterpret_cast<cx<float> *>(smem_raw);
     const int u = blockIdx.x;
     typename Acc::S *__restrict__ acc = aux + (size_t)u * N;
