@@ -39,73 +39,6 @@ namespace updc {
 #endif
 constexpr int CT_ROW_NT = UPDC_CT_ROW_NT;
 
-// Evict-first (ld.global.cs) load of a complex value read once: the column
-// kernels' input spectra and OTF columns, so the L2 keeps X-hat and the FP64
-// accumulator (forward y 0.54 -> 0.52 ms, adjoint 0.85 -> 0.83 ms on the
-// 5040-point columns of the 8 x 2048^2 -> 4096^2 field).
-__device__ __forceinline__ cx<float> ldcs_cx(const cx<float> *p) {
-    const float2 v = __ldcs(reinterpret_cast<const float2 *>(p));
-    return {v.x, v.y};
-}
-
-// L2 evict-last accesses (createpolicy + .L2::cache_hint) of the data a
-// kernel re-reads while it streams read-once inputs past it: the column
-// adjoint's FP64 accumulator (adjoint 0.83 -> 0.75 ms on the 5040-point
-// columns of the 8 x 2048^2 -> 4096^2 field) and the weighted ratio plane
-// the fused gather reads at random (1.16 -> 1.14 ms).
-__device__ __forceinline__ uint64_t l2_evict_last_policy() {
-    uint64_t p;
-    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
-    return p;
-}
-template <typename S> __device__ __forceinline__ S ld_keep(const S *p) {
-    if constexpr (sizeof(S) == 16) {
-        double a, b;
-        asm volatile("ld.global.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
-                     : "=d"(a), "=d"(b)
-                     : "l"(p), "l"(l2_evict_last_policy()));
-        S r;
-        memcpy(&r, &a, 8);
-        memcpy(reinterpret_cast<char *>(&r) + 8, &b, 8);
-        return r;
-    } else if constexpr (sizeof(S) == 8) {
-        float a, b;
-        asm volatile("ld.global.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;"
-                     : "=f"(a), "=f"(b)
-                     : "l"(p), "l"(l2_evict_last_policy()));
-        S r;
-        memcpy(&r, &a, 4);
-        memcpy(reinterpret_cast<char *>(&r) + 4, &b, 4);
-        return r;
-    } else {
-        return *p;
-    }
-}
-template <typename S> __device__ __forceinline__ void st_keep(S *p, const S &v) {
-    if constexpr (sizeof(S) == 16) {
-        double a, b;
-        memcpy(&a, &v, 8);
-        memcpy(&b, reinterpret_cast<const char *>(&v) + 8, 8);
-        asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(p), "d"(a), "d"(b),
-                     "l"(l2_evict_last_policy())
-                     : "memory");
-    } else if constexpr (sizeof(S) == 8) {
-        float a, b;
-        memcpy(&a, &v, 4);
-        memcpy(&b, reinterpret_cast<const char *>(&v) + 4, 4);
-        asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(p), "f"(a), "f"(b),
-                     "l"(l2_evict_last_policy())
-                     : "memory");
-    } else {
-        *p = v;
-    }
-}
-__device__ __forceinline__ float ld_keep_f(const float *p) {
-    float v;
-    asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(l2_evict_last_policy()));
-    return v;
-}
-
 // A compile-time radix list (the catalog's entries).
 template <int... R> struct CtRadices {
     static constexpr int n = CtProd<R...>::value;
